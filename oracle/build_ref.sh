@@ -1,0 +1,111 @@
+#!/usr/bin/env bash
+# Build the reference oracle from the UNMODIFIED reference sources.
+#
+# TEST INFRASTRUCTURE ONLY.  For each NCOL given (default: 2 3 4) this
+#   1. mirrors 4d_Q16/{include,susy,generic,libraries} as a symlink farm under
+#      oracle/_ref/n<NCOL>/ -- every file is a symlink to the reference except
+#      include/susy.h, which is regenerated with "#define NCOL <NCOL>" exactly
+#      as the reference's own testsuite/scalar/run_tests:11 sed-edits it;
+#   2. compiles the susy_hmc object set (susy/Make_template:155-159 plus the
+#      MY_OBJECTS/G_OBJECTS lists) and the complex/susy library routines with
+#      the reference's flags (susy/Make_scalar:7, libraries/Make_vanilla:9),
+#      plus -fPIC, linking oracle/lapack_min.c in place of -llapack -lblas;
+#   3. links oracle/_ref/n<NCOL>/susy_hmc (the reference program itself) and
+#      oracle/_ref/libsusyref_n<NCOL>.so (reference objects minus control.o,
+#      plus oracle/ref_harness.c) for ctypes.
+# Outputs go only to oracle/_ref/ (git-ignored, shipped with the tree).
+# The reference's own build system is not used.
+set -euo pipefail
+
+REF=${SUSY_REFERENCE:-/root/reference}/4d_Q16
+HERE=$(cd "$(dirname "$0")" && pwd)
+OUT=$HERE/_ref
+CC=${CC:-gcc}
+JOBS=${JOBS:-8}
+
+if [ ! -d "$REF/susy" ]; then
+  echo "build_ref.sh: reference sources not found at $REF" >&2
+  exit 2
+fi
+
+NCOLS=("$@")
+[ ${#NCOLS[@]} -eq 0 ] && NCOLS=(2 3 4)
+
+MY_OBJECTS="setup setup_lambda setup_offset action plaq ploop unit scalar_eig
+            link_trace widths determinant grsource utilities library_util
+            gauge_info congrad_multi"
+HMC_OBJECTS="update_o update_h setup_rhmc det_force"
+G_OBJECTS="io_helpers io_lat io_lat_utils make_lattice nersc_cksum ranstuff
+           gaugefix remap_stdio_from_args layout_hyper_prime io_ansi com_vanilla"
+LIB_OBJECTS="cmplx cexp clog csqrt ce_itheta dcmplx dcexp dclog dcsqrt dce_itheta
+             cmp_ahmat dump_ahmat make_ahmat uncmp_ahmat rand_ahmat
+             m_su2_mat_vec_n m_su2_mat_vec_a gaussrand z2rand byterevn m_mat_an
+             m_mat_na m_mat_nn realtr s_m_a_mat s_m_a_amat s_m_s_mat s_m_s_amat
+             adjoint mat_copy trace complextr dumpmat dumpsu2 clear_mat addmat
+             addamat submat subamat clearvec r_su2_hit_a l_su2_hit_n s_m_mat
+             s_m_amat s_a_d_mat cs_a_d_mat s_m_mat_nn s_m_mat_na s_m_mat_an
+             cs_m_mat cs_m_a_mat cs_m_a_amat cs_m_a_mata cs_m_s_mat"
+
+APP_FLAGS="-O3 -DP4 -Wall -fno-strict-aliasing -fPIC -DSINGLE -DPRECISION=2
+           -D_FILE_OFFSET_BITS=64 -D_LARGEFILE_SOURCE64
+           -DPHI_ALGORITHM -DHMC_ALGORITHM -w"
+LIB_FLAGS="-O3 -Wall -fPIC -DPRECISION=2 -w"
+
+build_one() {
+  local N=$1
+  local D=$OUT/n$N
+  mkdir -p "$D/obj"
+  for sub in include susy generic libraries; do
+    mkdir -p "$D/$sub"
+    for f in "$REF/$sub"/*.c "$REF/$sub"/*.h; do
+      [ -e "$f" ] || continue
+      local b
+      b=$(basename "$f")
+      [ "$sub/$b" = "include/susy.h" ] && continue
+      ln -sf "$f" "$D/$sub/$b"
+    done
+  done
+  sed -E "s/^(#define NCOL) .*/\1 $N/" "$REF/include/susy.h" > "$D/include/susy.h.tmp"
+  if ! cmp -s "$D/include/susy.h.tmp" "$D/include/susy.h" 2>/dev/null; then
+    mv "$D/include/susy.h.tmp" "$D/include/susy.h"
+  else
+    rm -f "$D/include/susy.h.tmp"
+  fi
+
+  local objs=() pids=()
+  compile() {   # src out flags...
+    local src=$1 out=$2
+    shift 2
+    if [ ! -e "$out" ] || [ "$src" -nt "$out" ] || [ "$D/include/susy.h" -nt "$out" ]; then
+      $CC -c "$@" "$src" -o "$out"
+    fi
+  }
+  for o in $MY_OBJECTS $HMC_OBJECTS; do
+    compile "$D/susy/$o.c" "$D/obj/$o.o" $APP_FLAGS -I"$D/susy" &
+    objs+=("$D/obj/$o.o")
+  done
+  for o in $G_OBJECTS; do
+    compile "$D/generic/$o.c" "$D/obj/g_$o.o" $APP_FLAGS -I"$D/susy" &
+    objs+=("$D/obj/g_$o.o")
+  done
+  for o in $LIB_OBJECTS; do
+    compile "$D/libraries/$o.c" "$D/obj/l_$o.o" $LIB_FLAGS &
+    objs+=("$D/obj/l_$o.o")
+  done
+  compile "$D/susy/control.c" "$D/obj/control.o" $APP_FLAGS -I"$D/susy" &
+  compile "$HERE/lapack_min.c" "$D/obj/lapack_min.o" -O2 -fPIC -Wall &
+  # The harness is project code compiled against the reference headers
+  ln -sf "$HERE/ref_harness.c" "$D/susy/zz_ref_harness.c"
+  compile "$D/susy/zz_ref_harness.c" "$D/obj/ref_harness.o" $APP_FLAGS -I"$D/susy" &
+  wait
+
+  $CC -o "$D/susy_hmc" "$D/obj/control.o" "${objs[@]}" "$D/obj/lapack_min.o" -lm
+  $CC -shared -o "$OUT/libsusyref_n$N.so" "$D/obj/ref_harness.o" "${objs[@]}" \
+      "$D/obj/lapack_min.o" -lm
+  echo "built $D/susy_hmc and $OUT/libsusyref_n$N.so"
+}
+
+mkdir -p "$OUT"
+for N in "${NCOLS[@]}"; do
+  build_one "$N"
+done
