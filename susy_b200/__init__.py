@@ -1,0 +1,9 @@
+"""susy_b200: B200-native RHMC fermion path of SUSY LATTICE (4d_Q16).
+
+The compute path is ``libsusy_b200.so`` (hand-written sm_100a CUDA behind
+the C ABI in include/susy_b200.h).  This package holds the Python mirror of
+the reference interface (:class:`Lattice`) and seeded synthetic inputs.
+"""
+from .lattice import Lattice, DeviceTF, SusyError, load_library, LIB_PATH  # noqa: F401
+
+__all__ = ["Lattice", "DeviceTF", "SusyError", "load_library", "LIB_PATH"]

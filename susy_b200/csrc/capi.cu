@@ -1,0 +1,409 @@
+// C ABI (include/susy_b200.h): lattice handle, host <-> device transfers,
+// fermion operator, DSq and the multi-shift CG driver.
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <cmath>
+#include <vector>
+#include "../../include/susy_b200.h"
+#include "kernels.h"
+#include "lattice.h"
+
+using namespace susy;
+
+namespace susy {
+
+static size_t mat_c(const susy_b200_lattice* h) { return (size_t)h->N * h->N; }
+
+bool ck(susy_b200_lattice* h, cudaError_t e) {
+  if (e == cudaSuccess) return true;
+  if (h && h->err == 0) h->err = SUSY_B200_ECUDA;
+  if (h) h->cuda_err = (int)e;
+  return false;
+}
+
+int set_err(susy_b200_lattice* h, int code) {
+  if (h && h->err == 0) h->err = code;
+  return code;
+}
+
+void* dalloc(susy_b200_lattice* h, size_t bytes) {
+  void* p = nullptr;
+  if (cudaMalloc(&p, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    set_err(h, SUSY_B200_ENOMEM);
+    return nullptr;
+  }
+  cudaMemsetAsync(p, 0, bytes, h->stream);
+  return p;
+}
+
+size_t field_bytes(const susy_b200_lattice* h, int K, int prec) {
+  return (size_t)K * mat_c(h) * h->g.S * (prec == 64 ? sizeof(double2) : sizeof(float2));
+}
+
+// Host link-type array (strided) -> device SoA FP64 field of K matrices
+int upload_links(susy_b200_lattice* h, void* dev, const double* host, size_t stride, int K) {
+  const size_t row = (size_t)K * mat_c(h) * 2 * sizeof(double);
+  if (stride == 0) stride = row;
+  if (!ck(h, cudaMemcpy2DAsync(h->stage, row, host, stride, row, h->g.V,
+                               cudaMemcpyHostToDevice, h->stream)))
+    return SUSY_B200_ECUDA;
+  aos_to_soa(h->g, K, h->N, h->stage, dev, 64, h->stream);
+  return ck(h, cudaGetLastError()) ? SUSY_B200_OK : SUSY_B200_ECUDA;
+}
+
+int download_links(susy_b200_lattice* h, const void* dev, double* host, size_t stride, int K) {
+  const size_t row = (size_t)K * mat_c(h) * 2 * sizeof(double);
+  if (stride == 0) stride = row;
+  soa_to_aos(h->g, K, h->N, dev, h->stage, 64, h->stream);
+  if (!ck(h, cudaMemcpy2DAsync(host, stride, h->stage, row, row, h->g.V,
+                               cudaMemcpyDeviceToHost, h->stream)))
+    return SUSY_B200_ECUDA;
+  return ck(h, cudaStreamSynchronize(h->stream)) ? SUSY_B200_OK : SUSY_B200_ECUDA;
+}
+
+int refresh_derived(susy_b200_lattice* h) {
+  compute_uinv(h->g, h->N, h->U, h->det, h->Uinv, h->stream);
+  compute_plaqdet(h->g, h->det, h->pd, h->zw, h->stream);
+  compute_dmuumu(h->g, h->N, h->U, h->pd, h->G, h->D, h->stream);
+  compute_fmunu(h->g, h->N, h->U, h->F, h->stream);
+  refresh_low(h);
+  return ck(h, cudaGetLastError()) ? SUSY_B200_OK : SUSY_B200_ECUDA;
+}
+
+// FP32 copies of the operator's inputs
+void refresh_low(susy_b200_lattice* h) {
+  const long nm = 5L * mat_c(h) * h->g.S;
+  convert_field(nm, h->U, 64, h->U32, 32, h->stream);
+  convert_field(nm, h->Uinv, 64, h->Uinv32, 32, h->stream);
+  convert_field(25L * h->g.S, h->pd, 64, h->pd32, 32, h->stream);
+}
+
+void dev_fop(susy_b200_lattice* h, const void* src, void* dst, int sign, int prec,
+             const void* add, double addc, double* dot, const int* skip) {
+  if (prec == 64)
+    fermion_op<double>(h->g, h->N, h->U, h->Uinv, h->pd, src, dst, sign, h->G, add, addc, dot,
+                       skip, h->stream);
+  else
+    fermion_op<float>(h->g, h->N, h->U32, h->Uinv32, h->pd32, src, dst, sign, h->G, add, addc,
+                      dot, skip, h->stream);
+}
+
+void* scratch_tf(susy_b200_lattice* h, int which, int prec) {
+  void** slot = prec == 64 ? &h->tf64[which] : &h->tf32[which];
+  if (!*slot) *slot = dalloc(h, field_bytes(h, NTF, prec));
+  return *slot;
+}
+
+double* partials(susy_b200_lattice* h, int which) {
+  if (!h->part[which]) {
+    const long n = (long)NTF * mat_c(h) * h->g.S;
+    size_t np = std::max((size_t)fop_partials(h->g), (size_t)vec_blocks(n)) + 64;
+    h->part[which] = (double*)dalloc(h, np * sizeof(double));
+  }
+  return h->part[which];
+}
+
+long tf_complex(const susy_b200_lattice* h) { return (long)NTF * mat_c(h) * h->g.S; }
+
+}  // namespace susy
+
+// ===========================================================================
+extern "C" {
+
+susy_b200_lattice* susy_b200_create(const susy_b200_params* p) {
+  // Even extents >= 2: the reference's parity-ordered site layout
+  // (layout_hyper_prime.c:157-170) is a bijection only then.
+  if (!p || p->ncol < 2 || p->ncol > 4 || p->nx < 2 || p->ny < 2 || p->nz < 2 || p->nt < 2 ||
+      (p->nx | p->ny | p->nz | p->nt) & 1 || (p->pbc != 1 && p->pbc != -1))
+    return nullptr;
+  if (cudaSetDevice(p->device) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  susy_b200_lattice* h = new susy_b200_lattice();
+  h->prm = *p;
+  h->N = p->ncol;
+  h->G = p->G;
+  h->g.nx = p->nx;
+  h->g.ny = p->ny;
+  h->g.nz = p->nz;
+  h->g.nt = p->nt;
+  h->g.V = p->nx * p->ny * p->nz * p->nt;
+  h->g.S = (h->g.V + 31) / 32 * 32;
+  h->g.pbc = p->pbc;
+  if (cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
+    cudaGetLastError();
+    delete h;
+    return nullptr;
+  }
+  h->stream = h->own_stream;
+  const size_t m5 = field_bytes(h, 5, 64);
+  h->U = dalloc(h, m5);
+  h->mom = dalloc(h, m5);
+  h->Uinv = dalloc(h, m5);
+  h->force = dalloc(h, m5);
+  h->det = dalloc(h, 5 * h->g.S * sizeof(double2));
+  h->pd = dalloc(h, 25 * h->g.S * sizeof(double2));
+  h->zw = dalloc(h, 25 * h->g.S * sizeof(double2));
+  h->D = dalloc(h, field_bytes(h, 1, 64));
+  h->F = dalloc(h, field_bytes(h, 10, 64));
+  h->U32 = dalloc(h, field_bytes(h, 5, 32));
+  h->Uinv32 = dalloc(h, field_bytes(h, 5, 32));
+  h->pd32 = dalloc(h, 25 * h->g.S * sizeof(float2));
+  h->stage = dalloc(h, (size_t)h->g.V * NTF * mat_c(h) * 2 * sizeof(double));
+  h->ms = (MsState*)dalloc(h, sizeof(MsState));
+  if (h->err) {
+    susy_b200_destroy(h);
+    return nullptr;
+  }
+  // Unit links until the caller sets some (coldlat, io_helpers.c:95)
+  std::vector<double> unit((size_t)h->g.V * 5 * mat_c(h) * 2, 0.0);
+  for (int s = 0; s < h->g.V; s++)
+    for (int a = 0; a < 5; a++)
+      for (int i = 0; i < h->N; i++)
+        unit[(((size_t)s * 5 + a) * mat_c(h) + i * h->N + i) * 2] = 1.0;
+  susy_b200_set_links(h, unit.data(), 0);
+  cudaStreamSynchronize(h->stream);
+  if (h->err) {
+    susy_b200_destroy(h);
+    return nullptr;
+  }
+  return h;
+}
+
+void susy_b200_destroy(susy_b200_lattice* h) {
+  if (!h) return;
+  cudaStreamSynchronize(h->stream);
+  void* ptrs[] = {h->U, h->mom, h->Uinv, h->force, h->det, h->pd, h->zw, h->D, h->F,
+                  h->U32, h->Uinv32, h->pd32, h->stage, h->ms};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+  for (int i = 0; i < SUSY_NSCRATCH; i++) {
+    if (h->tf64[i]) cudaFree(h->tf64[i]);
+    if (h->tf32[i]) cudaFree(h->tf32[i]);
+  }
+  for (int i = 0; i < SUSY_NPART; i++)
+    if (h->part[i]) cudaFree(h->part[i]);
+  for (std::vector<void*>* v : {&h->extra, &h->sols, &h->pvec64, &h->pvec32})
+    for (void* p : *v)
+      if (p) cudaFree(p);
+  if (h->poll) cudaFreeHost(h->poll);
+  if (h->own_stream) cudaStreamDestroy(h->own_stream);
+  delete h;
+}
+
+int susy_b200_last_error(const susy_b200_lattice* h) { return h ? h->err : SUSY_B200_EINVAL; }
+
+const char* susy_b200_error_string(int code) {
+  switch (code) {
+    case SUSY_B200_OK: return "ok";
+    case SUSY_B200_EINVAL: return "invalid argument";
+    case SUSY_B200_ECUDA: return "CUDA runtime error";
+    case SUSY_B200_ENOMEM: return "device allocation failed";
+    case SUSY_B200_ENOCONV: return "solver did not converge";
+    case SUSY_B200_ENAN: return "non-finite value";
+    default: return "unknown error";
+  }
+}
+
+int susy_b200_set_stream(susy_b200_lattice* h, void* s) {
+  if (!h) return SUSY_B200_EINVAL;
+  h->stream = s ? (cudaStream_t)s : h->own_stream;
+  return SUSY_B200_OK;
+}
+
+int susy_b200_sync(susy_b200_lattice* h) {
+  if (!h) return SUSY_B200_EINVAL;
+  return ck(h, cudaStreamSynchronize(h->stream)) ? SUSY_B200_OK : SUSY_B200_ECUDA;
+}
+
+int susy_b200_volume(const susy_b200_lattice* h) { return h ? h->g.V : 0; }
+
+int susy_b200_set_links(susy_b200_lattice* h, const double* links, size_t stride) {
+  if (!h || !links) return set_err(h, SUSY_B200_EINVAL);
+  int r = upload_links(h, h->U, links, stride, 5);
+  if (r) return r;
+  return refresh_derived(h);
+}
+
+int susy_b200_get_links(susy_b200_lattice* h, double* links, size_t stride) {
+  if (!h || !links) return set_err(h, SUSY_B200_EINVAL);
+  return download_links(h, h->U, links, stride, 5);
+}
+
+int susy_b200_set_mom(susy_b200_lattice* h, const double* mom, size_t stride) {
+  if (!h || !mom) return set_err(h, SUSY_B200_EINVAL);
+  return upload_links(h, h->mom, mom, stride, 5);
+}
+
+int susy_b200_get_mom(susy_b200_lattice* h, double* mom, size_t stride) {
+  if (!h || !mom) return set_err(h, SUSY_B200_EINVAL);
+  return download_links(h, h->mom, mom, stride, 5);
+}
+
+int susy_b200_compute_plaqdet(susy_b200_lattice* h) {
+  if (!h) return SUSY_B200_EINVAL;
+  compute_uinv(h->g, h->N, h->U, h->det, h->Uinv, h->stream);
+  compute_plaqdet(h->g, h->det, h->pd, h->zw, h->stream);
+  refresh_low(h);
+  return ck(h, cudaGetLastError()) ? SUSY_B200_OK : SUSY_B200_ECUDA;
+}
+
+int susy_b200_compute_Uinv(susy_b200_lattice* h) {
+  if (!h) return SUSY_B200_EINVAL;
+  compute_uinv(h->g, h->N, h->U, h->det, h->Uinv, h->stream);
+  refresh_low(h);
+  return ck(h, cudaGetLastError()) ? SUSY_B200_OK : SUSY_B200_ECUDA;
+}
+
+int susy_b200_compute_DmuUmu(susy_b200_lattice* h) {
+  if (!h) return SUSY_B200_EINVAL;
+  compute_dmuumu(h->g, h->N, h->U, h->pd, h->G, h->D, h->stream);
+  return ck(h, cudaGetLastError()) ? SUSY_B200_OK : SUSY_B200_ECUDA;
+}
+
+int susy_b200_compute_Fmunu(susy_b200_lattice* h) {
+  if (!h) return SUSY_B200_EINVAL;
+  compute_fmunu(h->g, h->N, h->U, h->F, h->stream);
+  return ck(h, cudaGetLastError()) ? SUSY_B200_OK : SUSY_B200_ECUDA;
+}
+
+int susy_b200_get_derived(susy_b200_lattice* h, double* plaqdet, double* DmuUmu, double* Fmunu,
+                          double* Uinv) {
+  if (!h) return SUSY_B200_EINVAL;
+  int r = 0;
+  if (plaqdet) {
+    // pd is 25 complex per site: a "field" of 25 1x1 matrices
+    Geo g = h->g;
+    std::vector<double> tmp((size_t)g.V * 25 * 2);
+    // reuse the generic converter with N = 1, K = 25
+    soa_to_aos(g, 25, 1, h->pd, h->stage, 64, h->stream);
+    if (!ck(h, cudaMemcpyAsync(plaqdet, h->stage, tmp.size() * sizeof(double),
+                               cudaMemcpyDeviceToHost, h->stream)))
+      return SUSY_B200_ECUDA;
+  }
+  if (DmuUmu && (r = download_links(h, h->D, DmuUmu, 0, 1))) return r;
+  if (Fmunu && (r = download_links(h, h->F, Fmunu, 0, 10))) return r;
+  if (Uinv && (r = download_links(h, h->Uinv, Uinv, 0, 5))) return r;
+  return ck(h, cudaStreamSynchronize(h->stream)) ? SUSY_B200_OK : SUSY_B200_ECUDA;
+}
+
+// ---- device-resident Twist_Fermion fields ---------------------------------
+size_t susy_b200_tf_bytes(const susy_b200_lattice* h, int prec) {
+  return h ? field_bytes(h, NTF, prec) : 0;
+}
+
+void* susy_b200_tf_alloc(susy_b200_lattice* h, int prec) {
+  if (!h || (prec != 64 && prec != 32)) return nullptr;
+  return dalloc(h, field_bytes(h, NTF, prec));
+}
+
+void susy_b200_tf_free(susy_b200_lattice* h, void* dev) {
+  if (h && dev) {
+    cudaStreamSynchronize(h->stream);
+    cudaFree(dev);
+  }
+}
+
+int susy_b200_tf_upload(susy_b200_lattice* h, void* dev, int prec, const double* host) {
+  if (!h || !dev || !host) return set_err(h, SUSY_B200_EINVAL);
+  const size_t bytes = (size_t)h->g.V * NTF * mat_c(h) * 2 * sizeof(double);
+  if (!ck(h, cudaMemcpyAsync(h->stage, host, bytes, cudaMemcpyHostToDevice, h->stream)))
+    return SUSY_B200_ECUDA;
+  aos_to_soa(h->g, NTF, h->N, h->stage, dev, prec, h->stream);
+  return ck(h, cudaGetLastError()) ? SUSY_B200_OK : SUSY_B200_ECUDA;
+}
+
+int susy_b200_tf_download(susy_b200_lattice* h, const void* dev, int prec, double* host) {
+  if (!h || !dev || !host) return set_err(h, SUSY_B200_EINVAL);
+  const size_t bytes = (size_t)h->g.V * NTF * mat_c(h) * 2 * sizeof(double);
+  soa_to_aos(h->g, NTF, h->N, dev, h->stage, prec, h->stream);
+  if (!ck(h, cudaMemcpyAsync(host, h->stage, bytes, cudaMemcpyDeviceToHost, h->stream)))
+    return SUSY_B200_ECUDA;
+  return ck(h, cudaStreamSynchronize(h->stream)) ? SUSY_B200_OK : SUSY_B200_ECUDA;
+}
+
+int susy_b200_tf_convert(susy_b200_lattice* h, const void* src, int ps, void* dst, int pd) {
+  if (!h || !src || !dst) return set_err(h, SUSY_B200_EINVAL);
+  convert_field(tf_complex(h), src, ps, dst, pd, h->stream);
+  return ck(h, cudaGetLastError()) ? SUSY_B200_OK : SUSY_B200_ECUDA;
+}
+
+int susy_b200_dev_fermion_op(susy_b200_lattice* h, const void* src, void* dst, int sign,
+                             int prec) {
+  if (!h || !src || !dst) return set_err(h, SUSY_B200_EINVAL);
+  if (sign != 1 && sign != -1) return set_err(h, SUSY_B200_EINVAL);
+  if (prec != 64 && prec != 32) return set_err(h, SUSY_B200_EINVAL);
+  dev_fop(h, src, dst, sign, prec, nullptr, 0.0, nullptr, nullptr);
+  return ck(h, cudaGetLastError()) ? SUSY_B200_OK : SUSY_B200_ECUDA;
+}
+
+int susy_b200_dev_DSq(susy_b200_lattice* h, const void* src, void* dst, int prec) {
+  if (!h || !src || !dst) return set_err(h, SUSY_B200_EINVAL);
+  if (prec != 64 && prec != 32) return set_err(h, SUSY_B200_EINVAL);
+  void* tmp = scratch_tf(h, 0, prec);
+  if (!tmp) return SUSY_B200_ENOMEM;
+  const double fm2 = h->prm.fmass > 1e-8 ? h->prm.fmass * h->prm.fmass : 0.0;
+  dev_fop(h, src, tmp, 1, prec, nullptr, 0.0, nullptr, nullptr);
+  dev_fop(h, tmp, dst, -1, prec, fm2 != 0.0 ? src : nullptr, fm2, nullptr, nullptr);
+  return ck(h, cudaGetLastError()) ? SUSY_B200_OK : SUSY_B200_ECUDA;
+}
+
+int susy_b200_fermion_op(susy_b200_lattice* h, const double* src, double* dest, int sign) {
+  if (!h || !src || !dest) return set_err(h, SUSY_B200_EINVAL);
+  if (sign != 1 && sign != -1) return set_err(h, SUSY_B200_EINVAL);
+  void* a = scratch_tf(h, 1, 64);
+  void* b = scratch_tf(h, 2, 64);
+  if (!a || !b) return SUSY_B200_ENOMEM;
+  int r = susy_b200_tf_upload(h, a, 64, src);
+  if (r) return r;
+  if ((r = susy_b200_dev_fermion_op(h, a, b, sign, 64))) return r;
+  return susy_b200_tf_download(h, b, 64, dest);
+}
+
+int susy_b200_DSq(susy_b200_lattice* h, const double* src, double* dest) {
+  if (!h || !src || !dest) return set_err(h, SUSY_B200_EINVAL);
+  void* a = scratch_tf(h, 1, 64);
+  void* b = scratch_tf(h, 2, 64);
+  if (!a || !b) return SUSY_B200_ENOMEM;
+  int r = susy_b200_tf_upload(h, a, 64, src);
+  if (r) return r;
+  if ((r = susy_b200_dev_DSq(h, a, b, 64))) return r;
+  return susy_b200_tf_download(h, b, 64, dest);
+}
+
+int susy_b200_dev_congrad_multi(susy_b200_lattice* h, const void* src, void* const* psim,
+                                int norder, const double* shift, int MaxCG, double errormin,
+                                double* size_r, int* iters) {
+  if (!h || !src || !psim || !shift || norder < 1 || norder > MS_MAXS)
+    return set_err(h, SUSY_B200_EINVAL);
+  return multishift_fp64(h, src, psim, norder, shift, MaxCG, errormin, size_r, iters);
+}
+
+int susy_b200_congrad_multi(susy_b200_lattice* h, const double* src, double* const* psim,
+                            int norder, const double* shift, int MaxCG, double errormin,
+                            double* size_r) {
+  if (!h || !src || !psim || !shift || norder < 1 || norder > MS_MAXS)
+    return set_err(h, SUSY_B200_EINVAL);
+  void* s = scratch_tf(h, 1, 64);
+  if (!s) return SUSY_B200_ENOMEM;
+  int r = susy_b200_tf_upload(h, s, 64, src);
+  if (r) return r;
+  std::vector<void*> ps(norder);
+  for (int j = 0; j < norder; j++) {
+    ps[j] = sol_field(h, j);
+    if (!ps[j]) return SUSY_B200_ENOMEM;
+  }
+  int it = 0;
+  double sr = 0.0;
+  r = multishift_fp64(h, s, ps.data(), norder, shift, MaxCG, errormin, &sr, &it);
+  if (r) return r;
+  for (int j = 0; j < norder; j++)
+    if ((r = susy_b200_tf_download(h, ps[j], 64, psim[j]))) return r;
+  if (size_r) *size_r = sr;
+  return it;
+}
+
+}  // extern "C"

@@ -1,0 +1,248 @@
+// Multi-shift conjugate gradient on (D^dag D + fmass^2 + shift_j), the
+// reference's congrad_multi (4d_Q16/susy/congrad_multi.c:26-221): zero
+// initial guess, Jegerlehner recurrences for the shifted systems, shift j
+// frozen once zeta_j^2 |r|^2 <= errormin |src|^2, stop when |r|^2 of the
+// base system reaches errormin |src|^2 or MaxCG iterations.
+//
+// Everything stays on the device.  The scalar recurrences run in FP64 in
+// one-block kernels that read the FP64 block partials of the two inner
+// products, so an iteration needs no host round trip; the host only polls
+// the state every few iterations.  Per iteration:
+//   fermion_op(+1)              tmp = D p0
+//   fermion_op(-1, epilogue)    mp = D^dag tmp + (fmass^2 + shift_0) p0,
+//                               partials of Re<p0, mp>
+//   k_ms_scalars1               beta_0 = -|r|^2 / <p0, mp>, zeta/beta_j
+//   k_ms_update_a               psi_j -= beta_j p_j; r += beta_0 mp;
+//                               partials of |r|^2
+//   k_ms_scalars2               alpha_j, freeze test, scroll
+//   k_ms_update_b               p_j = zeta_j r + alpha_j p_j
+// Vectors are FP64 (VT = double2) for the reference-faithful solver or FP32
+// (float2) for the low-precision pass of the mixed solver.
+#include "common.cuh"
+#include "kernels.h"
+
+namespace susy {
+
+constexpr int UT = 256;
+constexpr int ST = 256;
+
+__global__ void k_ms_init(MsState* st, const double* partials, int np, int maxcg,
+                          double errormin) {
+  __shared__ double sh[ST];
+  double v = 0.0;
+  for (int i = threadIdx.x; i < np; i += ST) v += partials[i];
+  sh[threadIdx.x] = v;
+  __syncthreads();
+  for (int o = ST / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    const double sn = sh[0];
+    st->source_norm = sn;
+    st->rsq = sn;
+    st->rsqstop = errormin * sn;
+    st->iter = 0;
+    st->maxcg = maxcg;
+    for (int j = 0; j < st->nshift; j++) {
+      st->zeta_im1[j] = 1.0;
+      st->zeta_i[j] = 1.0;
+      st->zeta_ip1[j] = 1.0;
+      st->alpha[j] = 0.0;
+      st->beta_im1[j] = 1.0;
+      st->beta_i[j] = 0.0;
+      st->converged[j] = 0;
+      st->active_p[j] = 1;
+    }
+    st->skip = (st->rsq <= st->rsqstop || maxcg <= 0) ? 1 : 0;
+    st->skip_b = 1;
+  }
+}
+
+SUSY_D double block_reduce_all(double v, double* sh) {
+  sh[threadIdx.x] = v;
+  __syncthreads();
+  for (int o = ST / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+    __syncthreads();
+  }
+  return sh[0];
+}
+
+__global__ void k_ms_scalars1(MsState* st, const double* partials, int np) {
+  __shared__ double sh[ST];
+  if (st->skip) {
+    if (threadIdx.x == 0) st->skip_b = 1;
+    return;
+  }
+  double v = 0.0;
+  for (int i = threadIdx.x; i < np; i += ST) v += partials[i];
+  const double cd = block_reduce_all(v, sh);
+  if (threadIdx.x != 0) return;
+  st->skip_b = 0;
+  st->cd = cd;
+  st->iter += 1;
+  const double b0 = -st->rsq / cd;
+  st->beta_i[0] = b0;
+  st->zeta_ip1[0] = 1.0;
+  const double s0 = st->shift[0];
+  for (int j = 1; j < st->nshift; j++) {
+    if (st->converged[j]) continue;
+    double z = st->zeta_i[j] * st->zeta_im1[j] * st->beta_im1[0];
+    const double c1 = b0 * st->alpha[0] * (st->zeta_im1[j] - st->zeta_i[j]);
+    const double c2 = st->zeta_im1[j] * st->beta_im1[0] * (1.0 - (st->shift[j] - s0) * b0);
+    z /= c1 + c2;
+    st->zeta_ip1[j] = z;
+    st->beta_i[j] = b0 * z / st->zeta_i[j];
+  }
+}
+
+__global__ void k_ms_scalars2(MsState* st, const double* partials, int np) {
+  __shared__ double sh[ST];
+  if (st->skip) return;
+  double v = 0.0;
+  for (int i = threadIdx.x; i < np; i += ST) v += partials[i];
+  const double rsqnew = block_reduce_all(v, sh);
+  if (threadIdx.x != 0) return;
+  const double a0 = rsqnew / st->rsq;
+  st->alpha[0] = a0;
+  st->active_p[0] = 1;
+  for (int j = 1; j < st->nshift; j++) {
+    st->active_p[j] = !st->converged[j];
+    if (st->converged[j]) continue;
+    st->alpha[j] = a0 * st->zeta_ip1[j] * st->beta_i[j] / (st->zeta_i[j] * st->beta_i[0]);
+  }
+  st->rsq = rsqnew;
+  for (int j = 1; j < st->nshift; j++) {
+    if (st->converged[j]) continue;
+    if (rsqnew * st->zeta_ip1[j] * st->zeta_ip1[j] <= st->rsqstop) st->converged[j] = 1;
+  }
+  for (int j = 0; j < st->nshift; j++) {
+    if (st->converged[j]) continue;
+    st->beta_im1[j] = st->beta_i[j];
+    st->zeta_im1[j] = st->zeta_i[j];
+    st->zeta_i[j] = st->zeta_ip1[j];
+  }
+  st->skip = (rsqnew <= st->rsqstop || st->iter >= st->maxcg) ? 1 : 0;
+}
+
+// psi_j -= beta_j p_j (j = 0 and every live shift), r += beta_0 mp, |r|^2
+template <typename VT>
+__global__ void __launch_bounds__(UT) k_ms_update_a(MsState* st, MsVecs v, long n, double* part) {
+  __shared__ double sb[MS_MAXS];
+  __shared__ int sc[MS_MAXS];
+  if (st->skip) return;
+  const int ns = st->nshift;
+  if (threadIdx.x < ns) {
+    sb[threadIdx.x] = st->beta_i[threadIdx.x];
+    sc[threadIdx.x] = threadIdx.x == 0 ? 0 : st->converged[threadIdx.x];
+  }
+  __syncthreads();
+  const long i = (long)blockIdx.x * UT + threadIdx.x;
+  double acc = 0.0;
+  if (i < n) {
+    const VT* mp = (const VT*)v.mp;
+    VT* r = (VT*)v.r;
+#pragma unroll 1
+    for (int j = 0; j < ns; j++) {
+      if (sc[j]) continue;
+      const VT pj = ((const VT*)v.p[j])[i];
+      VT* pp = (VT*)v.psi[j] + i;
+      VT x = *pp;
+      x.x -= sb[j] * pj.x;
+      x.y -= sb[j] * pj.y;
+      *pp = x;
+    }
+    VT rr = r[i];
+    const VT m = mp[i];
+    rr.x += sb[0] * m.x;
+    rr.y += sb[0] * m.y;
+    r[i] = rr;
+    acc = (double)rr.x * rr.x + (double)rr.y * rr.y;
+  }
+  acc = block_sum<UT>(acc);
+  if (threadIdx.x == 0) part[blockIdx.x] = acc;
+}
+
+// p_j = zeta_ip1_j r + alpha_j p_j for the shifts that were live
+template <typename VT>
+__global__ void __launch_bounds__(UT) k_ms_update_b(MsState* st, MsVecs v, long n) {
+  __shared__ double sz[MS_MAXS], sa[MS_MAXS];
+  __shared__ int sc[MS_MAXS];
+  if (st->skip_b) return;
+  const int ns = st->nshift;
+  if (threadIdx.x < ns) {
+    sz[threadIdx.x] = st->zeta_ip1[threadIdx.x];
+    sa[threadIdx.x] = st->alpha[threadIdx.x];
+    sc[threadIdx.x] = st->active_p[threadIdx.x];
+  }
+  __syncthreads();
+  const long i = (long)blockIdx.x * UT + threadIdx.x;
+  if (i >= n) return;
+  const VT r = ((const VT*)v.r)[i];
+#pragma unroll 1
+  for (int j = 0; j < ns; j++) {
+    if (!sc[j]) continue;
+    VT* pp = (VT*)v.p[j] + i;
+    VT p = *pp;
+    p.x = sz[j] * r.x + sa[j] * p.x;
+    p.y = sz[j] * r.y + sa[j] * p.y;
+    *pp = p;
+  }
+}
+
+// |x|^2 partials over n complex entries
+template <typename VT>
+__global__ void __launch_bounds__(UT) k_norm2(const VT* x, long n, double* part) {
+  const long i = (long)blockIdx.x * UT + threadIdx.x;
+  double acc = 0.0;
+  if (i < n) {
+    const VT a = x[i];
+    acc = (double)a.x * a.x + (double)a.y * a.y;
+  }
+  acc = block_sum<UT>(acc);
+  if (threadIdx.x == 0) part[blockIdx.x] = acc;
+}
+
+int vec_blocks(long n) { return (int)((n + UT - 1) / UT); }
+
+void ms_init(MsState* st, const void* src, int prec, long n, double* part, int maxcg,
+             double errormin, cudaStream_t s) {
+  const int nb = vec_blocks(n);
+  if (prec == 64)
+    k_norm2<double2><<<nb, UT, 0, s>>>((const double2*)src, n, part);
+  else
+    k_norm2<float2><<<nb, UT, 0, s>>>((const float2*)src, n, part);
+  k_ms_init<<<1, ST, 0, s>>>(st, part, nb, maxcg, errormin);
+}
+
+void ms_scalars1(MsState* st, const double* part, int np, cudaStream_t s) {
+  k_ms_scalars1<<<1, ST, 0, s>>>(st, part, np);
+}
+
+void ms_scalars2(MsState* st, const double* part, int np, cudaStream_t s) {
+  k_ms_scalars2<<<1, ST, 0, s>>>(st, part, np);
+}
+
+void ms_update_a(MsState* st, const MsVecs& v, int prec, long n, double* part, cudaStream_t s) {
+  if (prec == 64)
+    k_ms_update_a<double2><<<vec_blocks(n), UT, 0, s>>>(st, v, n, part);
+  else
+    k_ms_update_a<float2><<<vec_blocks(n), UT, 0, s>>>(st, v, n, part);
+}
+
+void ms_update_b(MsState* st, const MsVecs& v, int prec, long n, cudaStream_t s) {
+  if (prec == 64)
+    k_ms_update_b<double2><<<vec_blocks(n), UT, 0, s>>>(st, v, n);
+  else
+    k_ms_update_b<float2><<<vec_blocks(n), UT, 0, s>>>(st, v, n);
+}
+
+void norm2_partials(const void* x, int prec, long n, double* part, cudaStream_t s) {
+  if (prec == 64)
+    k_norm2<double2><<<vec_blocks(n), UT, 0, s>>>((const double2*)x, n, part);
+  else
+    k_norm2<float2><<<vec_blocks(n), UT, 0, s>>>((const float2*)x, n, part);
+}
+
+}  // namespace susy

@@ -1,0 +1,52 @@
+// Internal definition of the opaque handle declared in include/susy_b200.h.
+#pragma once
+#include <vector>
+#include "../../include/susy_b200.h"
+#include "kernels.h"
+
+#define SUSY_NSCRATCH 8
+#define SUSY_NPART 4
+
+struct susy_b200_lattice {
+  susy_b200_params prm;
+  susy::Geo g;
+  int N = 2;
+  double G = 0.0;
+  cudaStream_t stream = nullptr, own_stream = nullptr;
+  // FP64 lattice fields (device layout, common.cuh)
+  void *U = nullptr, *mom = nullptr, *Uinv = nullptr, *force = nullptr;
+  void *det = nullptr, *pd = nullptr, *zw = nullptr, *D = nullptr, *F = nullptr;
+  // FP32 copies read by the FP32 operator
+  void *U32 = nullptr, *Uinv32 = nullptr, *pd32 = nullptr;
+  void* stage = nullptr;  // AoS staging buffer (one FP64 Twist_Fermion)
+  susy::MsState* ms = nullptr;
+  void* tf64[SUSY_NSCRATCH] = {};
+  void* tf32[SUSY_NSCRATCH] = {};
+  double* part[SUSY_NPART] = {};
+  std::vector<void*> sols;    // solutions for the host-facing CG
+  std::vector<void*> pvec64;  // p_j of the FP64 multi-shift CG
+  std::vector<void*> pvec32;
+  std::vector<void*> extra;   // other lazily allocated fields
+  int* poll = nullptr;        // pinned host words for solver polling
+  int err = 0, cuda_err = 0;
+};
+
+namespace susy {
+bool ck(susy_b200_lattice* h, cudaError_t e);
+int set_err(susy_b200_lattice* h, int code);
+void* dalloc(susy_b200_lattice* h, size_t bytes);
+size_t field_bytes(const susy_b200_lattice* h, int K, int prec);
+int upload_links(susy_b200_lattice* h, void* dev, const double* host, size_t stride, int K);
+int download_links(susy_b200_lattice* h, const void* dev, double* host, size_t stride, int K);
+int refresh_derived(susy_b200_lattice* h);
+void refresh_low(susy_b200_lattice* h);
+void dev_fop(susy_b200_lattice* h, const void* src, void* dst, int sign, int prec,
+             const void* add, double addc, double* dot, const int* skip);
+void* scratch_tf(susy_b200_lattice* h, int which, int prec);
+double* partials(susy_b200_lattice* h, int which);
+long tf_complex(const susy_b200_lattice* h);
+void* sol_field(susy_b200_lattice* h, int j);
+int multishift_fp64(susy_b200_lattice* h, const void* src, void* const* psim, int norder,
+                    const double* shift, int MaxCG, double errormin, double* size_r,
+                    int* iters);
+}  // namespace susy

@@ -1,0 +1,251 @@
+"""Python mirror of the reference's hot-path interface over the C ABI.
+
+The method names, argument meaning and error behaviour follow the reference
+C functions (4d_Q16/susy/susy_includes.h:23-105): ``fermion_op(src, dest,
+sign)``, ``DSq(src, dest)``, ``congrad_multi(src, psim, MaxCG, errormin)``,
+``fermion_force``, ``gauge_force``, ``update_u``, ``update`` ...  Host arrays
+are float64 in the reference's own memory layout (Twist_Fermion /
+link-matrix arrays over sites in node_index order, see include/susy_b200.h).
+Every call goes through ``libsusy_b200.so``; there is no CPU fallback: if
+the library or a GPU is missing, construction raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libsusy_b200.so")
+
+_dp = C.POINTER(C.c_double)
+_vp = C.c_void_p
+
+
+class SusyError(RuntimeError):
+    """Raised when the CUDA library reports an error."""
+
+
+class Params(C.Structure):
+    _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int), ("nt", C.c_int),
+                ("ncol", C.c_int), ("pbc", C.c_int), ("kappa", C.c_double),
+                ("bmass", C.c_double), ("fmass", C.c_double), ("kappa_u1", C.c_double),
+                ("G", C.c_double), ("iseed", C.c_int), ("device", C.c_int)]
+
+
+_lib = None
+
+
+def load_library(path: str = LIB_PATH):
+    """Load libsusy_b200.so and declare its C signatures (raises if absent)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise SusyError("libsusy_b200.so not built: run `python -m susy_b200.build`")
+    L = C.CDLL(path)
+    L.susy_b200_create.restype = _vp
+    L.susy_b200_create.argtypes = [C.POINTER(Params)]
+    L.susy_b200_destroy.argtypes = [_vp]
+    L.susy_b200_last_error.argtypes = [_vp]
+    L.susy_b200_error_string.restype = C.c_char_p
+    L.susy_b200_error_string.argtypes = [C.c_int]
+    L.susy_b200_set_stream.argtypes = [_vp, _vp]
+    L.susy_b200_sync.argtypes = [_vp]
+    L.susy_b200_volume.argtypes = [_vp]
+    for name in ("set_links", "get_links", "set_mom", "get_mom"):
+        getattr(L, "susy_b200_" + name).argtypes = [_vp, _dp, C.c_size_t]
+    for name in ("compute_plaqdet", "compute_Uinv", "compute_DmuUmu", "compute_Fmunu"):
+        getattr(L, "susy_b200_" + name).argtypes = [_vp]
+    L.susy_b200_get_derived.argtypes = [_vp, _dp, _dp, _dp, _dp]
+    L.susy_b200_fermion_op.argtypes = [_vp, _dp, _dp, C.c_int]
+    L.susy_b200_DSq.argtypes = [_vp, _dp, _dp]
+    L.susy_b200_congrad_multi.argtypes = [_vp, _dp, C.POINTER(_dp), C.c_int, _dp, C.c_int,
+                                          C.c_double, _dp]
+    L.susy_b200_tf_alloc.restype = _vp
+    L.susy_b200_tf_alloc.argtypes = [_vp, C.c_int]
+    L.susy_b200_tf_free.argtypes = [_vp, _vp]
+    L.susy_b200_tf_bytes.restype = C.c_size_t
+    L.susy_b200_tf_bytes.argtypes = [_vp, C.c_int]
+    L.susy_b200_tf_upload.argtypes = [_vp, _vp, C.c_int, _dp]
+    L.susy_b200_tf_download.argtypes = [_vp, _vp, C.c_int, _dp]
+    L.susy_b200_tf_convert.argtypes = [_vp, _vp, C.c_int, _vp, C.c_int]
+    L.susy_b200_dev_fermion_op.argtypes = [_vp, _vp, _vp, C.c_int, C.c_int]
+    L.susy_b200_dev_DSq.argtypes = [_vp, _vp, _vp, C.c_int]
+    L.susy_b200_dev_congrad_multi.argtypes = [_vp, _vp, C.POINTER(_vp), C.c_int, _dp, C.c_int,
+                                              C.c_double, _dp, C.POINTER(C.c_int)]
+    _lib = L
+    return L
+
+
+def _ptr(a: np.ndarray):
+    if a.dtype != np.float64 or not a.flags["C_CONTIGUOUS"]:
+        raise TypeError("expected a C-contiguous float64 array")
+    return a.ctypes.data_as(_dp)
+
+
+class DeviceTF:
+    """A Twist_Fermion field resident on the GPU (FP64 or FP32)."""
+
+    def __init__(self, lat: "Lattice", prec: int = 64):
+        self.lat = lat
+        self.prec = prec
+        self.ptr = lat.lib.susy_b200_tf_alloc(lat.h, prec)
+        if not self.ptr:
+            lat._check(-3)
+
+    def upload(self, host: np.ndarray):
+        self.lat._check(self.lat.lib.susy_b200_tf_upload(self.lat.h, self.ptr, self.prec,
+                                                         _ptr(host)))
+
+    def download(self, out: np.ndarray | None = None) -> np.ndarray:
+        if out is None:
+            out = np.zeros(self.lat.tf_doubles)
+        self.lat._check(self.lat.lib.susy_b200_tf_download(self.lat.h, self.ptr, self.prec,
+                                                           _ptr(out)))
+        return out
+
+    def free(self):
+        if self.ptr:
+            self.lat.lib.susy_b200_tf_free(self.lat.h, self.ptr)
+            self.ptr = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+class Lattice:
+    """One lattice on one GPU, mirroring the reference's global-state API."""
+
+    def __init__(self, dims, ncol, pbc=-1, lam=1.0, bmass=0.0, fmass=0.0, kappa_u1=0.0,
+                 G=0.0, iseed=41, device=0):
+        self.lib = load_library()
+        nx, ny, nz, nt = dims
+        self.dims = tuple(dims)
+        self.N = ncol
+        self.prm = Params(nx, ny, nz, nt, ncol, pbc, ncol * 0.25 / lam, bmass, fmass,
+                          kappa_u1, G, iseed, device)
+        self.lam = lam
+        h = self.lib.susy_b200_create(C.byref(self.prm))
+        if not h:
+            raise SusyError("susy_b200_create failed (no GPU, bad parameters or out of memory)")
+        self.h = h
+        self.V = self.lib.susy_b200_volume(h)
+        self.mat_doubles = 2 * ncol * ncol
+        self.tf_doubles = self.V * 16 * self.mat_doubles
+        self.link_doubles = self.V * 5 * self.mat_doubles
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.susy_b200_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc):
+        if rc is not None and rc < 0:
+            msg = self.lib.susy_b200_error_string(int(rc)).decode()
+            raise SusyError("susy_b200 error %d: %s" % (rc, msg))
+        return rc
+
+    def set_stream(self, stream_ptr: int | None):
+        self._check(self.lib.susy_b200_set_stream(self.h, stream_ptr))
+
+    def sync(self):
+        self._check(self.lib.susy_b200_sync(self.h))
+
+    # ---- fields ------------------------------------------------------------
+    def set_links(self, links: np.ndarray):
+        self._check(self.lib.susy_b200_set_links(self.h, _ptr(links), 0))
+
+    def get_links(self) -> np.ndarray:
+        out = np.zeros(self.link_doubles)
+        self._check(self.lib.susy_b200_get_links(self.h, _ptr(out), 0))
+        return out
+
+    def set_mom(self, mom: np.ndarray):
+        self._check(self.lib.susy_b200_set_mom(self.h, _ptr(mom), 0))
+
+    def get_mom(self) -> np.ndarray:
+        out = np.zeros(self.link_doubles)
+        self._check(self.lib.susy_b200_get_mom(self.h, _ptr(out), 0))
+        return out
+
+    def compute_plaqdet(self):
+        self._check(self.lib.susy_b200_compute_plaqdet(self.h))
+
+    def compute_Uinv(self):
+        self._check(self.lib.susy_b200_compute_Uinv(self.h))
+
+    def compute_DmuUmu(self):
+        self._check(self.lib.susy_b200_compute_DmuUmu(self.h))
+
+    def compute_Fmunu(self):
+        self._check(self.lib.susy_b200_compute_Fmunu(self.h))
+
+    def derived(self):
+        """(plaqdet [V*25*2], DmuUmu, Fmunu, Uinv) in reference order."""
+        pd = np.zeros(self.V * 50)
+        D = np.zeros(self.V * self.mat_doubles)
+        F = np.zeros(self.V * 10 * self.mat_doubles)
+        Ui = np.zeros(self.link_doubles)
+        self._check(self.lib.susy_b200_get_derived(self.h, _ptr(pd), _ptr(D), _ptr(F), _ptr(Ui)))
+        return pd, D, F, Ui
+
+    # ---- operators ---------------------------------------------------------
+    def fermion_op(self, src: np.ndarray, dest: np.ndarray, sign: int):
+        """fermion_op(src, dest, sign), utilities.c:765; sign must be +-1."""
+        if sign not in (1, -1):
+            raise ValueError("Error: incorrect sign in fermion_op: %r" % (sign,))
+        self._check(self.lib.susy_b200_fermion_op(self.h, _ptr(src), _ptr(dest), int(sign)))
+
+    def DSq(self, src: np.ndarray, dest: np.ndarray):
+        """DSq(src, dest) = (D^dag D + fmass^2) src, utilities.c:874."""
+        self._check(self.lib.susy_b200_DSq(self.h, _ptr(src), _ptr(dest)))
+
+    def congrad_multi(self, src: np.ndarray, psim, shift, MaxCG: int, errormin: float):
+        """congrad_multi(src, psim, MaxCG, errormin, &size_r), congrad_multi.c:26.
+
+        psim: list of Norder output arrays.  Returns (iterations, size_r).
+        """
+        shift = np.ascontiguousarray(shift, dtype=np.float64)
+        n = len(shift)
+        arr = (_dp * n)(*[_ptr(p) for p in psim])
+        sr = C.c_double(0.0)
+        it = self.lib.susy_b200_congrad_multi(self.h, _ptr(src), arr, n, _ptr(shift),
+                                              int(MaxCG), float(errormin), C.byref(sr))
+        self._check(it)
+        return it, sr.value
+
+    # ---- device-resident variants -----------------------------------------
+    def tf(self, prec: int = 64) -> DeviceTF:
+        return DeviceTF(self, prec)
+
+    def dev_fermion_op(self, src: DeviceTF, dst: DeviceTF, sign: int):
+        self._check(self.lib.susy_b200_dev_fermion_op(self.h, src.ptr, dst.ptr, int(sign),
+                                                      src.prec))
+
+    def dev_DSq(self, src: DeviceTF, dst: DeviceTF):
+        self._check(self.lib.susy_b200_dev_DSq(self.h, src.ptr, dst.ptr, src.prec))
+
+    def dev_convert(self, src: DeviceTF, dst: DeviceTF):
+        self._check(self.lib.susy_b200_tf_convert(self.h, src.ptr, src.prec, dst.ptr, dst.prec))
+
+    def dev_congrad_multi(self, src: DeviceTF, psim, shift, MaxCG: int, errormin: float):
+        shift = np.ascontiguousarray(shift, dtype=np.float64)
+        n = len(shift)
+        arr = (_vp * n)(*[p.ptr for p in psim])
+        sr = C.c_double(0.0)
+        it = C.c_int(0)
+        self._check(self.lib.susy_b200_dev_congrad_multi(self.h, src.ptr, arr, n, _ptr(shift),
+                                                         int(MaxCG), float(errormin),
+                                                         C.byref(sr), C.byref(it)))
+        return it.value, sr.value

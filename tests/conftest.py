@@ -1,0 +1,12 @@
+"""Shared pytest set-up: repository root on sys.path and the gpu marker."""
+import os
+import sys
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200) and libsusy_b200.so")
+    config.addinivalue_line("markers", "slow: long-running CPU test")
