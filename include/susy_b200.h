@@ -117,10 +117,103 @@ int susy_b200_tf_convert(susy_b200_lattice *h, const void *src, int prec_src, vo
                          int prec_dst);
 int susy_b200_dev_fermion_op(susy_b200_lattice *h, const void *src, void *dst, int sign,
                              int prec);
+/* Operator kernel selection (no reference counterpart: the reference has one
+ * CPU loop nest).  autotune times every variant on this lattice and keeps
+ * the fastest per precision; it also runs by itself on first use.
+ * fop_variant returns the current variant of a precision, sets it when
+ * set_to >= 0 and copies the autotuner's ms per variant when ms != NULL. */
+int susy_b200_autotune(susy_b200_lattice *h);
+int susy_b200_fop_variant(susy_b200_lattice *h, int prec, int set_to, float *ms_per_variant);
 int susy_b200_dev_DSq(susy_b200_lattice *h, const void *src, void *dst, int prec);
 int susy_b200_dev_congrad_multi(susy_b200_lattice *h, const void *src, void *const *psim,
                                 int norder, const double *shift, int MaxCG, double errormin,
                                 double *size_r, int *iters);
+/* Same solve with the mixed-precision solver (FP32 multi-shift pass, then
+ * FP64 true-residual defect correction per shift): every shift ends with
+ * |src - (D^dag D + shift_j) psim_j|^2 <= errormin |src|^2 in FP64, unless
+ * MaxCG operator applications run out.  *size_r = worst final true |r|^2;
+ * *iters = operator applications (multi-shift pass plus refinement). */
+int susy_b200_dev_congrad_multi_mixed(susy_b200_lattice *h, const void *src, void *const *psim,
+                                      int norder, const double *shift, int MaxCG,
+                                      double errormin, double *size_r, int *iters);
+
+/* ---- forces, link update, actions ------------------------------------- */
+/* double gauge_force(Real eps)   susy/update_h.c:15 (includes det_force
+ * when kappa_u1 > 0, update_h.c:257); mom -= kappa eps f_U^dag;
+ * *norm = eps sqrt(sum |f|^2) / volume as the reference returns. */
+int susy_b200_gauge_force(susy_b200_lattice *h, double eps, double *norm);
+/* double det_force(Real eps)     susy/det_force.c:6; *norm = sum |f|^2 */
+int susy_b200_det_force(susy_b200_lattice *h, double eps, double *norm);
+/* double fermion_force(Real eps, Twist_Fermion *src, Twist_Fermion **sol)
+ *   susy/update_h.c:928; Norder and amp4[] (globals there) are arguments.
+ *   src is accepted and ignored, as in the reference. */
+int susy_b200_fermion_force(susy_b200_lattice *h, double eps, const double *src,
+                            const double *const *sol, int norder, const double *amp4,
+                            double *norm);
+int susy_b200_dev_fermion_force(susy_b200_lattice *h, double eps, void *const *sol, int norder,
+                                const double *amp4, double *norm);
+/* void update_u(Real eps)  susy/update_o.c:20: link += eps mom, then the
+ * derived fields are recomputed. */
+int susy_b200_update_u(susy_b200_lattice *h, double eps);
+/* double action(src, sol)  susy/action.c:293.  parts receives
+ * {gauge, bmass, det, fermion (summed over roots), mom}; sol holds
+ * nroot * norder arrays, root-major. */
+int susy_b200_action(susy_b200_lattice *h, int nroot, const double *const *src,
+                     const double *const *sol, int norder, const double *amp4, double ampdeg4,
+                     double *parts);
+
+/* ---- random fields (per-site generators, generic/ranstuff.c) ----------- */
+/* (Re)seed every site generator and the node generator as setup() does
+ * (make_lattice.c:48, setup.c:246); create() already seeds with p->iseed. */
+int susy_b200_seed(susy_b200_lattice *h, int iseed);
+/* void ranmom()   susy/grsource.c:44: fills the device momenta */
+int susy_b200_ranmom(susy_b200_lattice *h);
+/* Gaussian Twist_Fermion R in grsource's draw order (grsource.c:213-245) */
+int susy_b200_gaussian_tf(susy_b200_lattice *h, double *out);
+
+/* ---- RHMC trajectory ---------------------------------------------------- */
+#define SUSY_B200_SOLVER_FP64 0    /* congrad_multi as the reference runs it   */
+#define SUSY_B200_SOLVER_MIXED 1   /* FP32 multi-shift + FP64 residual refinement */
+#define SUSY_B200_MAX_NROOT 4
+
+/* Rational approximation and integrator parameters: the reference globals
+ * of susy/lattice.h:116-124 and setup_rhmc.c (amp4/shift4/amp8/shift8/
+ * ampdeg4/ampdeg8 for Norder poles), nsteps[2], traj_length, niter and
+ * rsqmin = error_per_site^2 (setup.c:356-359). */
+typedef struct {
+  int Nroot, Norder;
+  const double *amp4, *shift4, *amp8, *shift8;
+  double ampdeg4, ampdeg8;
+  int nsteps[2];
+  double traj_length;
+  int niter;
+  double rsqmin;
+  int solver;          /* SUSY_B200_SOLVER_FP64 or SUSY_B200_SOLVER_MIXED */
+  int no_metropolis;   /* 1: keep the end of every trajectory and only report
+                          delta S, as the reference's non-HMC build does
+                          (update_o.c:252-255) */
+} susy_b200_rhmc;
+
+/* What update() prints (update_o.c:244-277) */
+typedef struct {
+  double delta_S, start_S, end_S, xrandom;
+  double start_parts[5], end_parts[5];   /* gauge, bmass, det, fermion, mom */
+  int accept, iters;
+  double gnorm, max_gf;
+  double fnorm[SUSY_B200_MAX_NROOT], max_ff[SUSY_B200_MAX_NROOT];
+} susy_b200_traj;
+
+/* int grsource(Twist_Fermion *src)   susy/grsource.c:200; returns CG iterations */
+int susy_b200_grsource(susy_b200_lattice *h, const susy_b200_rhmc *r, double *src);
+/* int update()   susy/update_o.c:127: one HMC trajectory (momentum refresh,
+ * pseudofermions, Omelyan integration, Metropolis with the node generator).
+ * Returns the CG iteration count or a negative error code. */
+int susy_b200_update(susy_b200_lattice *h, const susy_b200_rhmc *r, susy_b200_traj *res);
+/* update() with the refreshed momenta and pseudofermion sources replaced by
+ * the given ones (mom: link-type array; src: Nroot Twist_Fermion arrays),
+ * to replay a trajectory from known fields. */
+int susy_b200_update_replay(susy_b200_lattice *h, const susy_b200_rhmc *r, susy_b200_traj *res,
+                            const double *mom, const double *const *src);
 
 #ifdef __cplusplus
 }

@@ -4,6 +4,8 @@ The compute path is ``libsusy_b200.so`` (hand-written sm_100a CUDA behind
 the C ABI in include/susy_b200.h).  This package holds the Python mirror of
 the reference interface (:class:`Lattice`) and seeded synthetic inputs.
 """
-from .lattice import Lattice, DeviceTF, SusyError, load_library, LIB_PATH  # noqa: F401
+from .lattice import (Lattice, DeviceTF, SusyError, RHMC, load_library, LIB_PATH,  # noqa: F401
+                      SOLVER_FP64, SOLVER_MIXED)
 
-__all__ = ["Lattice", "DeviceTF", "SusyError", "load_library", "LIB_PATH"]
+__all__ = ["Lattice", "DeviceTF", "SusyError", "RHMC", "load_library", "LIB_PATH",
+           "SOLVER_FP64", "SOLVER_MIXED"]

@@ -8,6 +8,7 @@
 #include "../../include/susy_b200.h"
 #include "kernels.h"
 #include "lattice.h"
+#include "hmc.h"
 
 using namespace susy;
 
@@ -80,14 +81,56 @@ void refresh_low(susy_b200_lattice* h) {
   convert_field(25L * h->g.S, h->pd, 64, h->pd32, 32, h->stream);
 }
 
-void dev_fop(susy_b200_lattice* h, const void* src, void* dst, int sign, int prec,
-             const void* add, double addc, double* dot, const int* skip) {
+static int launch_variant(susy_b200_lattice* h, const void* src, void* dst, int sign, int prec,
+                          const void* add, double addc, double* dot, const int* skip, int v) {
   if (prec == 64)
-    fermion_op<double>(h->g, h->N, h->U, h->Uinv, h->pd, src, dst, sign, h->G, add, addc, dot,
-                       skip, h->stream);
-  else
-    fermion_op<float>(h->g, h->N, h->U32, h->Uinv32, h->pd32, src, dst, sign, h->G, add, addc,
-                      dot, skip, h->stream);
+    return fermion_op<double>(h->g, h->N, h->U, h->Uinv, h->pd, src, dst, sign, h->G, add, addc,
+                              dot, skip, v, h->stream);
+  return fermion_op<float>(h->g, h->N, h->U32, h->Uinv32, h->pd32, src, dst, sign, h->G, add,
+                           addc, dot, skip, v, h->stream);
+}
+
+// Project-written autotuner: time one D^dag D with every kernel variant on
+// this lattice and keep the fastest for this precision.  Runs on the first
+// operator call of each precision (before any stream capture).
+int autotune_fop(susy_b200_lattice* h, int prec) {
+  const int pi = prec == 64 ? 0 : 1;
+  void* a = scratch_tf(h, 6, prec);
+  void* b = scratch_tf(h, 7, prec);
+  if (!a || !b) return SUSY_B200_ENOMEM;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  float best = 1e30f;
+  int bestv = FOP_MAT;
+  for (int v = 0; v < FOP_NVARIANTS; v++) {
+    launch_variant(h, a, b, 1, prec, nullptr, 0.0, nullptr, nullptr, v);
+    cudaEventRecord(e0, h->stream);
+    for (int r = 0; r < 3; r++) {
+      launch_variant(h, a, b, 1, prec, nullptr, 0.0, nullptr, nullptr, v);
+      launch_variant(h, b, a, -1, prec, nullptr, 0.0, nullptr, nullptr, v);
+    }
+    cudaEventRecord(e1, h->stream);
+    cudaEventSynchronize(e1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    h->fop_ms[pi][v] = ms / 3.f;
+    if (ms < best) {
+      best = ms;
+      bestv = v;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  h->fop_variant[pi] = bestv;
+  return ck(h, cudaGetLastError()) ? SUSY_B200_OK : SUSY_B200_ECUDA;
+}
+
+int dev_fop(susy_b200_lattice* h, const void* src, void* dst, int sign, int prec,
+            const void* add, double addc, double* dot, const int* skip) {
+  const int pi = prec == 64 ? 0 : 1;
+  if (h->fop_variant[pi] < 0) autotune_fop(h, prec);
+  return launch_variant(h, src, dst, sign, prec, add, addc, dot, skip, h->fop_variant[pi]);
 }
 
 void* scratch_tf(susy_b200_lattice* h, int which, int prec) {
@@ -158,6 +201,7 @@ susy_b200_lattice* susy_b200_create(const susy_b200_params* p) {
     susy_b200_destroy(h);
     return nullptr;
   }
+  node_prn_init(h->node_prn, p->iseed, h->g.V);
   // Unit links until the caller sets some (coldlat, io_helpers.c:95)
   std::vector<double> unit((size_t)h->g.V * 5 * mat_c(h) * 2, 0.0);
   for (int s = 0; s < h->g.V; s++)
@@ -177,7 +221,8 @@ void susy_b200_destroy(susy_b200_lattice* h) {
   if (!h) return;
   cudaStreamSynchronize(h->stream);
   void* ptrs[] = {h->U, h->mom, h->Uinv, h->force, h->det, h->pd, h->zw, h->D, h->F,
-                  h->U32, h->Uinv32, h->pd32, h->stage, h->ms};
+                  h->U32, h->Uinv32, h->pd32, h->stage, h->ms, h->bigpart, h->gen, h->prn,
+                  h->rng_bad, h->ptrbuf};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (int i = 0; i < SUSY_NSCRATCH; i++) {
@@ -186,7 +231,8 @@ void susy_b200_destroy(susy_b200_lattice* h) {
   }
   for (int i = 0; i < SUSY_NPART; i++)
     if (h->part[i]) cudaFree(h->part[i]);
-  for (std::vector<void*>* v : {&h->extra, &h->sols, &h->pvec64, &h->pvec32})
+  for (std::vector<void*>* v : {&h->extra, &h->sols, &h->pvec64, &h->pvec32, &h->gsrc,
+                                &h->gr_psim, &h->traj_psim, &h->extra5, &h->refine})
     for (void* p : *v)
       if (p) cudaFree(p);
   if (h->poll) cudaFreeHost(h->poll);
@@ -340,6 +386,21 @@ int susy_b200_dev_fermion_op(susy_b200_lattice* h, const void* src, void* dst, i
   return ck(h, cudaGetLastError()) ? SUSY_B200_OK : SUSY_B200_ECUDA;
 }
 
+int susy_b200_autotune(susy_b200_lattice* h) {
+  if (!h) return SUSY_B200_EINVAL;
+  int r = autotune_fop(h, 64);
+  return r ? r : autotune_fop(h, 32);
+}
+
+int susy_b200_fop_variant(susy_b200_lattice* h, int prec, int set_to, float* ms_per_variant) {
+  if (!h || (prec != 64 && prec != 32) || set_to >= FOP_NVARIANTS) return SUSY_B200_EINVAL;
+  const int pi = prec == 64 ? 0 : 1;
+  if (set_to >= 0) h->fop_variant[pi] = set_to;
+  if (ms_per_variant)
+    for (int v = 0; v < FOP_NVARIANTS; v++) ms_per_variant[v] = h->fop_ms[pi][v];
+  return h->fop_variant[pi];
+}
+
 int susy_b200_dev_DSq(susy_b200_lattice* h, const void* src, void* dst, int prec) {
   if (!h || !src || !dst) return set_err(h, SUSY_B200_EINVAL);
   if (prec != 64 && prec != 32) return set_err(h, SUSY_B200_EINVAL);
@@ -380,6 +441,14 @@ int susy_b200_dev_congrad_multi(susy_b200_lattice* h, const void* src, void* con
   if (!h || !src || !psim || !shift || norder < 1 || norder > MS_MAXS)
     return set_err(h, SUSY_B200_EINVAL);
   return multishift_fp64(h, src, psim, norder, shift, MaxCG, errormin, size_r, iters);
+}
+
+int susy_b200_dev_congrad_multi_mixed(susy_b200_lattice* h, const void* src, void* const* psim,
+                                      int norder, const double* shift, int MaxCG,
+                                      double errormin, double* size_r, int* iters) {
+  if (!h || !src || !psim || !shift || norder < 1 || norder > MS_MAXS)
+    return set_err(h, SUSY_B200_EINVAL);
+  return multishift_mixed(h, src, psim, norder, shift, MaxCG, errormin, size_r, iters);
 }
 
 int susy_b200_congrad_multi(susy_b200_lattice* h, const double* src, double* const* psim,

@@ -127,7 +127,8 @@ __global__ void k_ms_scalars2(MsState* st, const double* partials, int np) {
 }
 
 // psi_j -= beta_j p_j (j = 0 and every live shift), r += beta_0 mp, |r|^2
-template <typename VT>
+// VT: type of p, r, mp; XT: type of the solutions psi
+template <typename VT, typename XT>
 __global__ void __launch_bounds__(UT) k_ms_update_a(MsState* st, MsVecs v, long n, double* part) {
   __shared__ double sb[MS_MAXS];
   __shared__ int sc[MS_MAXS];
@@ -147,8 +148,8 @@ __global__ void __launch_bounds__(UT) k_ms_update_a(MsState* st, MsVecs v, long 
     for (int j = 0; j < ns; j++) {
       if (sc[j]) continue;
       const VT pj = ((const VT*)v.p[j])[i];
-      VT* pp = (VT*)v.psi[j] + i;
-      VT x = *pp;
+      XT* pp = (XT*)v.psi[j] + i;
+      XT x = *pp;
       x.x -= sb[j] * pj.x;
       x.y -= sb[j] * pj.y;
       *pp = x;
@@ -224,11 +225,65 @@ void ms_scalars2(MsState* st, const double* part, int np, cudaStream_t s) {
   k_ms_scalars2<<<1, ST, 0, s>>>(st, part, np);
 }
 
-void ms_update_a(MsState* st, const MsVecs& v, int prec, long n, double* part, cudaStream_t s) {
+void ms_update_a(MsState* st, const MsVecs& v, int prec, int prec_x, long n, double* part,
+                 cudaStream_t s) {
   if (prec == 64)
-    k_ms_update_a<double2><<<vec_blocks(n), UT, 0, s>>>(st, v, n, part);
+    k_ms_update_a<double2, double2><<<vec_blocks(n), UT, 0, s>>>(st, v, n, part);
+  else if (prec_x == 64)
+    k_ms_update_a<float2, double2><<<vec_blocks(n), UT, 0, s>>>(st, v, n, part);
   else
-    k_ms_update_a<float2><<<vec_blocks(n), UT, 0, s>>>(st, v, n, part);
+    k_ms_update_a<float2, float2><<<vec_blocks(n), UT, 0, s>>>(st, v, n, part);
+}
+
+// r64 = b - ax, r32 = (float) r64, partials of |r64|^2
+__global__ void __launch_bounds__(UT) k_residual(long n, const double2* b, const double2* ax,
+                                                 double2* r64, float2* r32, double* part) {
+  const long i = (long)blockIdx.x * UT + threadIdx.x;
+  double acc = 0.0;
+  if (i < n) {
+    const double2 u = b[i], w = ax[i];
+    const double2 r = make_double2(u.x - w.x, u.y - w.y);
+    if (r64) r64[i] = r;
+    if (r32) r32[i] = make_float2((float)r.x, (float)r.y);
+    acc = r.x * r.x + r.y * r.y;
+  }
+  acc = block_sum<UT>(acc);
+  if (threadIdx.x == 0) part[blockIdx.x] = acc;
+}
+
+// x64 += e32
+__global__ void k_add_low(long n, const float2* e, double2* x) {
+  const long i = (long)blockIdx.x * UT + threadIdx.x;
+  if (i >= n) return;
+  double2 v = x[i];
+  const float2 d = e[i];
+  v.x += d.x;
+  v.y += d.y;
+  x[i] = v;
+}
+
+__global__ void k_scale(long n, double s, double2* x) {
+  const long i = (long)blockIdx.x * UT + threadIdx.x;
+  if (i >= n) return;
+  double2 v = x[i];
+  v.x *= s;
+  v.y *= s;
+  x[i] = v;
+}
+
+int residual_partials(long n, const void* b, const void* ax, void* r64, void* r32, double* part,
+                      cudaStream_t s) {
+  k_residual<<<vec_blocks(n), UT, 0, s>>>(n, (const double2*)b, (const double2*)ax,
+                                          (double2*)r64, (float2*)r32, part);
+  return vec_blocks(n);
+}
+
+void add_low(long n, const void* e32, void* x64, cudaStream_t s) {
+  k_add_low<<<vec_blocks(n), UT, 0, s>>>(n, (const float2*)e32, (double2*)x64);
+}
+
+void scale_field(long n, double sc, void* x, cudaStream_t s) {
+  k_scale<<<vec_blocks(n), UT, 0, s>>>(n, sc, (double2*)x);
 }
 
 void ms_update_b(MsState* st, const MsVecs& v, int prec, long n, cudaStream_t s) {

@@ -20,43 +20,10 @@
 // Optional epilogue (used by DSq inside the CG): out += addc * add and a
 // per-block partial of Re<add, out> in FP64.
 #include "common.cuh"
+#include "fop.cuh"
 #include "kernels.h"
 
 namespace susy {
-
-template <typename R>
-struct FopArgs {
-  typedef typename CT<R>::T T;
-  Geo g;
-  const T* U;
-  const T* Uinv;
-  const T* pd;
-  const T* src;
-  T* dst;
-  R G;
-  int doG;
-  const T* add;
-  R addc;
-  double* dot;
-  const int* skip;  // device flag: nonzero = do nothing (finished solves)
-};
-
-constexpr int FOP_THREADS = 128;
-
-// The three link indices not in {A, B}, ascending
-template <int A, int B>
-struct Compl {
-  static constexpr int k(int n) {
-    int c = 0;
-    for (int v = 0; v < 5; v++) {
-      if (v == A || v == B) continue;
-      if (c == n) return v;
-      c++;
-    }
-    return -1;
-  }
-  static constexpr int K0 = k(0), K1 = k(1), K2 = k(2);
-};
 
 template <int N, typename R, int SIGN, int A, int B, int C, int P, int Q>
 SUSY_D void ptop_terms(Mat<N, R>& acc, const FopArgs<R>& a, const Site& c) {
@@ -223,8 +190,8 @@ SUSY_D Mat<N, R> site_out(const FopArgs<R>& a, const Site& c) {
   return acc;
 }
 
-template <int N, typename R, int SIGN>
-__global__ void __launch_bounds__(FOP_THREADS)
+template <int N, typename R, int SIGN, int MINB>
+__global__ void __launch_bounds__(FOP_THREADS, MINB)
 fermion_op_kernel(FopArgs<R> a) {
   if (a.skip && *a.skip) return;
   const int comp = blockIdx.x % NTF;
@@ -272,21 +239,24 @@ fermion_op_kernel(FopArgs<R> a) {
   }
 }
 
-template <int N, typename R>
-static void launch_fop(const FopArgs<R>& a, int sign, cudaStream_t st) {
+template <int N, typename R, int MINB>
+static int launch_fop(const FopArgs<R>& a, int sign, cudaStream_t st) {
   const int nblk = ((a.g.V + FOP_THREADS - 1) / FOP_THREADS) * NTF;
   if (sign > 0)
-    fermion_op_kernel<N, R, 1><<<nblk, FOP_THREADS, 0, st>>>(a);
+    fermion_op_kernel<N, R, 1, MINB><<<nblk, FOP_THREADS, 0, st>>>(a);
   else
-    fermion_op_kernel<N, R, -1><<<nblk, FOP_THREADS, 0, st>>>(a);
+    fermion_op_kernel<N, R, -1, MINB><<<nblk, FOP_THREADS, 0, st>>>(a);
+  return nblk;
 }
 
-int fop_partials(const Geo& g) { return ((g.V + FOP_THREADS - 1) / FOP_THREADS) * NTF; }
+// Upper bound on the dot partials any variant writes
+int fop_partials(const Geo& g) { return ((g.V + 31) / 32) * NTF; }
 
+// Launch one application; returns the number of dot partials written.
 template <typename R>
-void fermion_op(const Geo& g, int N, const void* U, const void* Uinv, const void* pd,
+int fermion_op(const Geo& g, int N, const void* U, const void* Uinv, const void* pd,
                 const void* src, void* dst, int sign, double G, const void* add,
-                double addc, double* dot, const int* skip, cudaStream_t st) {
+                double addc, double* dot, const int* skip, int variant, cudaStream_t st) {
   typedef typename CT<R>::T T;
   FopArgs<R> a;
   a.g = g;
@@ -301,18 +271,23 @@ void fermion_op(const Geo& g, int N, const void* U, const void* Uinv, const void
   a.addc = (R)addc;
   a.dot = dot;
   a.skip = skip;
+  if (variant == FOP_ROWS) return fermion_op_rows<R>(a, N, sign, st);
   switch (N) {
-    case 2: launch_fop<2, R>(a, sign, st); break;
-    case 3: launch_fop<3, R>(a, sign, st); break;
-    case 4: launch_fop<4, R>(a, sign, st); break;
+    case 2:
+      return variant == FOP_MAT_OCC ? launch_fop<2, R, 3>(a, sign, st)
+                                    : launch_fop<2, R, 1>(a, sign, st);
+    case 3:
+      return variant == FOP_MAT_OCC ? launch_fop<3, R, 2>(a, sign, st)
+                                    : launch_fop<3, R, 1>(a, sign, st);
+    default: return launch_fop<4, R, 1>(a, sign, st);
   }
 }
 
-template void fermion_op<double>(const Geo&, int, const void*, const void*, const void*,
+template int fermion_op<double>(const Geo&, int, const void*, const void*, const void*,
                                  const void*, void*, int, double, const void*, double,
-                                 double*, const int*, cudaStream_t);
-template void fermion_op<float>(const Geo&, int, const void*, const void*, const void*,
+                                 double*, const int*, int, cudaStream_t);
+template int fermion_op<float>(const Geo&, int, const void*, const void*, const void*,
                                 const void*, void*, int, double, const void*, double,
-                                double*, const int*, cudaStream_t);
+                                double*, const int*, int, cudaStream_t);
 
 }  // namespace susy

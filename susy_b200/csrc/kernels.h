@@ -26,11 +26,17 @@ struct MsVecs {
   void* mp;
 };
 
-// fermion_op.cu
+// fermion_op.cu, fermion_op_rows.cu
+// Kernel variants: matrix per thread, the same with a register cap for
+// occupancy, and one matrix row per thread.
+enum { FOP_MAT = 0, FOP_MAT_OCC = 1, FOP_ROWS = 2, FOP_NVARIANTS = 3 };
 template <typename R>
-void fermion_op(const Geo& g, int N, const void* U, const void* Uinv, const void* pd,
+int fermion_op(const Geo& g, int N, const void* U, const void* Uinv, const void* pd,
                 const void* src, void* dst, int sign, double G, const void* add, double addc,
-                double* dot, const int* skip, cudaStream_t st);
+                double* dot, const int* skip, int variant, cudaStream_t st);
+template <typename R> struct FopArgs;
+template <typename R>
+int fermion_op_rows(const FopArgs<R>& a, int N, int sign, cudaStream_t st);
 int fop_partials(const Geo& g);
 
 // derived.cu
@@ -52,8 +58,36 @@ void ms_init(MsState* st, const void* src, int prec, long n, double* part, int m
              double errormin, cudaStream_t s);
 void ms_scalars1(MsState* st, const double* part, int np, cudaStream_t s);
 void ms_scalars2(MsState* st, const double* part, int np, cudaStream_t s);
-void ms_update_a(MsState* st, const MsVecs& v, int prec, long n, double* part, cudaStream_t s);
+void ms_update_a(MsState* st, const MsVecs& v, int prec, int prec_x, long n, double* part,
+                 cudaStream_t s);
+int residual_partials(long n, const void* b, const void* ax, void* r64, void* r32, double* part,
+                      cudaStream_t s);
+void add_low(long n, const void* e32, void* x64, cudaStream_t s);
+void scale_field(long n, double sc, void* x, cudaStream_t s);
 void ms_update_b(MsState* st, const MsVecs& v, int prec, long n, cudaStream_t s);
 void norm2_partials(const void* x, int prec, long n, double* part, cudaStream_t s);
 
+}  // namespace susy
+
+namespace susy {
+// force.cu
+int force_blocks(const Geo& g);
+int site_blocks(const Geo& g);
+void fermion_force_pole(const Geo& g, int N, const void* U, const void* Uinv, const void* pd,
+                        const void* sol, const void* psol, void* force, double amp, double G,
+                        cudaStream_t st);
+int mom_sub(long n, const void* force, void* mom, double eps, double* part, cudaStream_t st);
+void axpy_field(long n, double s, const void* x, void* y, cudaStream_t st);
+int gauge_force(const Geo& g, int N, const void* U, const void* Uinv, const void* pd,
+                const void* zw, const void* D, const void* F, void* mom, double G, double bmass,
+                double kappa, double kappa_u1, double eps, int det_only, double* part,
+                cudaStream_t st);
+int action_partials(const Geo& g, int N, const void* U, const void* D, const void* F,
+                    const void* pd, const void* mom, double* part, cudaStream_t st);
+int fermion_action_partials(long n, const void* src, int nsol, const void* const* sol_dev_array,
+                            const double* amp_dev, double ampdeg, double* part, cudaStream_t st);
+// rng.cu
+void init_prn(const Geo& g, int seed, void* st, cudaStream_t s);
+void gauss_fill(const Geo& g, int N, void* st, const void* gen, int K, int gen_outer, void* out,
+                int* bad, cudaStream_t s);
 }  // namespace susy

@@ -4,6 +4,13 @@
 #include "../../include/susy_b200.h"
 #include "kernels.h"
 
+namespace susy {
+// Host copy of the reference's node generator (ranstuff.c:22-63)
+struct HostPrn {
+  uint32_t r[7], mult, add, ic;
+};
+}  // namespace susy
+
 #define SUSY_NSCRATCH 8
 #define SUSY_NPART 4
 
@@ -28,6 +35,17 @@ struct susy_b200_lattice {
   std::vector<void*> pvec32;
   std::vector<void*> extra;   // other lazily allocated fields
   int* poll = nullptr;        // pinned host words for solver polling
+  // trajectory state (hmc.cu)
+  double* bigpart = nullptr;
+  long bigpart_n = 0;
+  void* gen = nullptr;        // U(N) generators
+  void* prn = nullptr;        // per-site generator states
+  int* rng_bad = nullptr;
+  void* ptrbuf = nullptr;     // device copy of field pointers / coefficients
+  std::vector<void*> gsrc, gr_psim, traj_psim, extra5, refine;
+  susy::HostPrn node_prn = {};
+  int fop_variant[2] = {-1, -1};  // chosen operator kernel (FP64, FP32); -1 = tune
+  float fop_ms[2][8] = {};        // autotuner timings per variant
   int err = 0, cuda_err = 0;
 };
 
@@ -40,8 +58,9 @@ int upload_links(susy_b200_lattice* h, void* dev, const double* host, size_t str
 int download_links(susy_b200_lattice* h, const void* dev, double* host, size_t stride, int K);
 int refresh_derived(susy_b200_lattice* h);
 void refresh_low(susy_b200_lattice* h);
-void dev_fop(susy_b200_lattice* h, const void* src, void* dst, int sign, int prec,
-             const void* add, double addc, double* dot, const int* skip);
+int dev_fop(susy_b200_lattice* h, const void* src, void* dst, int sign, int prec,
+            const void* add, double addc, double* dot, const int* skip);
+int autotune_fop(susy_b200_lattice* h, int prec);
 void* scratch_tf(susy_b200_lattice* h, int which, int prec);
 double* partials(susy_b200_lattice* h, int which);
 long tf_complex(const susy_b200_lattice* h);

@@ -27,6 +27,54 @@ class SusyError(RuntimeError):
     """Raised when the CUDA library reports an error."""
 
 
+class RHMCParams(C.Structure):
+    """susy_b200_rhmc: rational approximation and integrator settings."""
+    _fields_ = [("Nroot", C.c_int), ("Norder", C.c_int), ("amp4", _dp), ("shift4", _dp),
+                ("amp8", _dp), ("shift8", _dp), ("ampdeg4", C.c_double),
+                ("ampdeg8", C.c_double), ("nsteps", C.c_int * 2), ("traj_length", C.c_double),
+                ("niter", C.c_int), ("rsqmin", C.c_double), ("solver", C.c_int),
+                ("no_metropolis", C.c_int)]
+
+
+class TrajResult(C.Structure):
+    _fields_ = [("delta_S", C.c_double), ("start_S", C.c_double), ("end_S", C.c_double),
+                ("xrandom", C.c_double), ("start_parts", C.c_double * 5),
+                ("end_parts", C.c_double * 5), ("accept", C.c_int), ("iters", C.c_int),
+                ("gnorm", C.c_double), ("max_gf", C.c_double), ("fnorm", C.c_double * 4),
+                ("max_ff", C.c_double * 4)]
+
+
+SOLVER_FP64 = 0
+SOLVER_MIXED = 1
+
+
+class RHMC:
+    """Owns the coefficient arrays behind a RHMCParams structure."""
+
+    def __init__(self, Norder=15, Nroot=1, nstep=5, nstep_gauge=4, traj_length=1.0,
+                 niter=5000, error_per_site=1e-5, solver=SOLVER_FP64, tables=None,
+                 no_metropolis=False):
+        if tables is None:
+            from .rhmc_tables import rhmc
+            tables = rhmc(Norder, Nroot)
+        self.t = {k: (np.ascontiguousarray(v, dtype=np.float64) if isinstance(v, list) else v)
+                  for k, v in tables.items()}
+        self.p = RHMCParams()
+        self.p.Nroot = Nroot
+        self.p.Norder = Norder
+        for k in ("amp4", "shift4", "amp8", "shift8"):
+            setattr(self.p, k, self.t[k].ctypes.data_as(_dp))
+        self.p.ampdeg4 = self.t["ampdeg4"]
+        self.p.ampdeg8 = self.t["ampdeg8"]
+        self.p.nsteps[0] = nstep
+        self.p.nsteps[1] = nstep_gauge
+        self.p.traj_length = traj_length
+        self.p.niter = niter
+        self.p.rsqmin = error_per_site * error_per_site   # setup.c:356-359
+        self.p.solver = solver
+        self.p.no_metropolis = int(no_metropolis)
+
+
 class Params(C.Structure):
     _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int), ("nt", C.c_int),
                 ("ncol", C.c_int), ("pbc", C.c_int), ("kappa", C.c_double),
@@ -73,8 +121,29 @@ def load_library(path: str = LIB_PATH):
     L.susy_b200_tf_convert.argtypes = [_vp, _vp, C.c_int, _vp, C.c_int]
     L.susy_b200_dev_fermion_op.argtypes = [_vp, _vp, _vp, C.c_int, C.c_int]
     L.susy_b200_dev_DSq.argtypes = [_vp, _vp, _vp, C.c_int]
+    L.susy_b200_autotune.argtypes = [_vp]
+    L.susy_b200_fop_variant.argtypes = [_vp, C.c_int, C.c_int, C.POINTER(C.c_float)]
     L.susy_b200_dev_congrad_multi.argtypes = [_vp, _vp, C.POINTER(_vp), C.c_int, _dp, C.c_int,
                                               C.c_double, _dp, C.POINTER(C.c_int)]
+    L.susy_b200_dev_congrad_multi_mixed.argtypes = [_vp, _vp, C.POINTER(_vp), C.c_int, _dp,
+                                                    C.c_int, C.c_double, _dp,
+                                                    C.POINTER(C.c_int)]
+    L.susy_b200_update_u.argtypes = [_vp, C.c_double]
+    L.susy_b200_gauge_force.argtypes = [_vp, C.c_double, _dp]
+    L.susy_b200_det_force.argtypes = [_vp, C.c_double, _dp]
+    L.susy_b200_fermion_force.argtypes = [_vp, C.c_double, _dp, C.POINTER(_dp), C.c_int, _dp,
+                                          _dp]
+    L.susy_b200_dev_fermion_force.argtypes = [_vp, C.c_double, C.POINTER(_vp), C.c_int, _dp,
+                                              _dp]
+    L.susy_b200_action.argtypes = [_vp, C.c_int, C.POINTER(_dp), C.POINTER(_dp), C.c_int, _dp,
+                                   C.c_double, _dp]
+    L.susy_b200_seed.argtypes = [_vp, C.c_int]
+    L.susy_b200_ranmom.argtypes = [_vp]
+    L.susy_b200_gaussian_tf.argtypes = [_vp, _dp]
+    L.susy_b200_grsource.argtypes = [_vp, C.POINTER(RHMCParams), _dp]
+    L.susy_b200_update.argtypes = [_vp, C.POINTER(RHMCParams), C.POINTER(TrajResult)]
+    L.susy_b200_update_replay.argtypes = [_vp, C.POINTER(RHMCParams), C.POINTER(TrajResult),
+                                          _dp, C.POINTER(_dp)]
     _lib = L
     return L
 
@@ -225,6 +294,92 @@ class Lattice:
         self._check(it)
         return it, sr.value
 
+    # ---- forces, link update, actions (update_h.c, update_o.c, action.c) ---
+    def gauge_force(self, eps: float) -> float:
+        n = C.c_double(0.0)
+        self._check(self.lib.susy_b200_gauge_force(self.h, float(eps), C.byref(n)))
+        return n.value
+
+    def det_force(self, eps: float) -> float:
+        n = C.c_double(0.0)
+        self._check(self.lib.susy_b200_det_force(self.h, float(eps), C.byref(n)))
+        return n.value
+
+    def fermion_force(self, eps: float, src, sol, amp4) -> float:
+        amp4 = np.ascontiguousarray(amp4, dtype=np.float64)
+        arr = (_dp * len(sol))(*[_ptr(x) for x in sol])
+        n = C.c_double(0.0)
+        self._check(self.lib.susy_b200_fermion_force(self.h, float(eps),
+                                                     None if src is None else _ptr(src), arr,
+                                                     len(sol), _ptr(amp4), C.byref(n)))
+        return n.value
+
+    def update_u(self, eps: float):
+        self._check(self.lib.susy_b200_update_u(self.h, float(eps)))
+
+    def action(self, srcs=(), sols=(), amp4=None, ampdeg4=0.0):
+        """(gauge, bmass, det, fermion, mom) as action.c:293 sums them."""
+        parts = np.zeros(5)
+        nroot = len(srcs)
+        norder = len(sols[0]) if nroot else 0
+        a = np.ascontiguousarray(amp4 if amp4 is not None else [0.0], dtype=np.float64)
+        sarr = (_dp * max(nroot, 1))(*[_ptr(x) for x in srcs])
+        flat = [x for row in sols for x in row]
+        parr = (_dp * max(len(flat), 1))(*[_ptr(x) for x in flat])
+        self._check(self.lib.susy_b200_action(self.h, nroot, sarr, parr, norder, _ptr(a),
+                                              float(ampdeg4), _ptr(parts)))
+        return parts
+
+    # ---- random fields and the trajectory ---------------------------------
+    def seed(self, iseed: int):
+        self._check(self.lib.susy_b200_seed(self.h, int(iseed)))
+
+    def ranmom(self):
+        self._check(self.lib.susy_b200_ranmom(self.h))
+
+    def gaussian_tf(self) -> np.ndarray:
+        out = np.zeros(self.tf_doubles)
+        self._check(self.lib.susy_b200_gaussian_tf(self.h, _ptr(out)))
+        return out
+
+    def grsource(self, rhmc: RHMC):
+        out = np.zeros(self.tf_doubles)
+        it = self._check(self.lib.susy_b200_grsource(self.h, C.byref(rhmc.p), _ptr(out)))
+        return out, it
+
+    @staticmethod
+    def _traj(res: TrajResult) -> dict:
+        return dict(delta_S=res.delta_S, start=res.start_S, end=res.end_S,
+                    xrandom=res.xrandom, accept=bool(res.accept), iters=res.iters,
+                    start_parts=list(res.start_parts), end_parts=list(res.end_parts),
+                    gnorm=res.gnorm, max_gf=res.max_gf, fnorm=list(res.fnorm),
+                    max_ff=list(res.max_ff))
+
+    def update(self, rhmc: RHMC) -> dict:
+        """One HMC trajectory, update_o.c:127."""
+        res = TrajResult()
+        self._check(self.lib.susy_b200_update(self.h, C.byref(rhmc.p), C.byref(res)))
+        return self._traj(res)
+
+    def update_replay(self, rhmc: RHMC, mom: np.ndarray | None, srcs) -> dict:
+        res = TrajResult()
+        arr = None
+        if srcs is not None:
+            arr = (_dp * len(srcs))(*[_ptr(x) for x in srcs])
+        self._check(self.lib.susy_b200_update_replay(self.h, C.byref(rhmc.p), C.byref(res),
+                                                     None if mom is None else _ptr(mom), arr))
+        return self._traj(res)
+
+    # ---- operator kernel selection -----------------------------------------
+    def autotune(self):
+        self._check(self.lib.susy_b200_autotune(self.h))
+
+    def fop_variant(self, prec: int = 64, set_to: int = -1):
+        """(current variant, autotuner ms per variant) for one precision."""
+        ms = (C.c_float * 8)()
+        v = self._check(self.lib.susy_b200_fop_variant(self.h, prec, set_to, ms))
+        return v, [ms[i] for i in range(3)]
+
     # ---- device-resident variants -----------------------------------------
     def tf(self, prec: int = 64) -> DeviceTF:
         return DeviceTF(self, prec)
@@ -239,13 +394,16 @@ class Lattice:
     def dev_convert(self, src: DeviceTF, dst: DeviceTF):
         self._check(self.lib.susy_b200_tf_convert(self.h, src.ptr, src.prec, dst.ptr, dst.prec))
 
-    def dev_congrad_multi(self, src: DeviceTF, psim, shift, MaxCG: int, errormin: float):
+    def dev_congrad_multi(self, src: DeviceTF, psim, shift, MaxCG: int, errormin: float,
+                          mixed: bool = False):
+        """Solve on device fields; mixed=True uses the mixed-precision solver."""
         shift = np.ascontiguousarray(shift, dtype=np.float64)
         n = len(shift)
         arr = (_vp * n)(*[p.ptr for p in psim])
         sr = C.c_double(0.0)
         it = C.c_int(0)
-        self._check(self.lib.susy_b200_dev_congrad_multi(self.h, src.ptr, arr, n, _ptr(shift),
-                                                         int(MaxCG), float(errormin),
-                                                         C.byref(sr), C.byref(it)))
+        fn = (self.lib.susy_b200_dev_congrad_multi_mixed if mixed
+              else self.lib.susy_b200_dev_congrad_multi)
+        self._check(fn(self.h, src.ptr, arr, n, _ptr(shift), int(MaxCG), float(errormin),
+                       C.byref(sr), C.byref(it)))
         return it.value, sr.value

@@ -1,0 +1,194 @@
+"""GPU parity of forces, actions, random fields and the HMC trajectory.
+
+Reference functions: gauge_force / det_force (update_h.c:15, det_force.c:6),
+fermion_force (update_h.c:928), update_u (update_o.c:20), action pieces
+(action.c:106-286), ranmom / grsource draws (grsource.c:44,200), update()
+(update_o.c:127).  The oracle is oracle/susy_np.py on identical inputs.
+Tolerances: FP64 fields 1e-12 relative (max-norm); force norms and actions
+1e-12 relative; Gaussian fields 1e-12 (device log() may round differently
+from libm in the last bit); the trajectory's delta S to 1e-7 absolute with
+the same accept decision and iteration count within +-2 per solve.
+"""
+import numpy as np
+import pytest
+
+from oracle import susy_np as O
+from susy_b200 import Lattice, RHMC, SOLVER_FP64, SOLVER_MIXED
+from susy_b200 import synth
+from susy_b200.rhmc_tables import rhmc as rhmc_table
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    return float(np.abs(a - b).max() / np.abs(b).max())
+
+
+def make(dims, N, seed=3, noise=0.2, **kw):
+    U = synth.links(dims, N, noise, seed)
+    lat = Lattice(dims, N, pbc=-1, **kw)
+    lat.set_links(synth.to_ref(dims, U))
+    geo = O.Geometry(dims, -1)
+    prm = O.Params(lam=kw.get("lam", 1.0), bmass=kw.get("bmass", 0.0),
+                   fmass=kw.get("fmass", 0.0), kappa_u1=kw.get("kappa_u1", 0.0),
+                   G=kw.get("G", 0.0), N=N)
+    return lat, geo, prm, U
+
+
+@pytest.mark.parametrize("N", [2, 3])
+def test_gauge_force(N):
+    dims = (4, 4, 4, 4)
+    lat, geo, prm, U = make(dims, N, lam=1.5, bmass=0.3, G=0.05, kappa_u1=0.4)
+    der = O.compute_derived(geo, prm, U)
+    mom0 = synth.links(dims, N, 0.5, 9) - np.eye(N)
+    lat.set_mom(synth.to_ref(dims, mom0))
+    mom = mom0.copy()
+    want = O.gauge_force(geo, prm, U, der, mom, 0.07)
+    got = lat.gauge_force(0.07)
+    assert abs(got - want) <= 1e-12 * abs(want)
+    assert rel(synth.from_ref(dims, lat.get_mom(), 5, N), mom) < 1e-12
+
+
+def test_det_force():
+    dims, N = (4, 4, 4, 4), 2
+    lat, geo, prm, U = make(dims, N, kappa_u1=0.7, G=0.05)
+    der = O.compute_derived(geo, prm, U)
+    mom = np.zeros_like(U)
+    lat.set_mom(synth.to_ref(dims, mom))
+    want = O.det_force(geo, prm, U, der, mom, 0.05)
+    got = lat.det_force(0.05)
+    assert abs(got - want) <= 1e-12 * abs(want)
+    assert rel(synth.from_ref(dims, lat.get_mom(), 5, N), mom) < 1e-12
+
+
+@pytest.mark.parametrize("N,G", [(2, 0.05), (3, 0.05), (2, 0.0)])
+def test_fermion_force(N, G):
+    dims = (4, 4, 4, 4)
+    lat, geo, prm, U = make(dims, N, G=G, bmass=0.2)
+    der = O.compute_derived(geo, prm, U)
+    sols = [synth.tf_source(dims, N, 40 + k) for k in range(3)]
+    amp = np.array([0.3, 1.7, 0.02])
+    mom = np.zeros_like(U)
+    lat.set_mom(synth.to_ref(dims, mom))
+    want = O.fermion_force(geo, prm, U, der, mom, 0.11, sols, amp)
+    got = lat.fermion_force(0.11, None, [synth.to_ref(dims, s) for s in sols], amp)
+    assert abs(got - want) <= 1e-12 * abs(want)
+    assert rel(synth.from_ref(dims, lat.get_mom(), 5, N), mom) < 1e-12
+
+
+def test_update_u_and_derived():
+    dims, N = (4, 4, 4, 4), 3
+    lat, geo, prm, U = make(dims, N, G=0.05)
+    mom = synth.links(dims, N, 0.3, 12) - np.eye(N)
+    lat.set_mom(synth.to_ref(dims, mom))
+    lat.update_u(0.13)
+    U2 = U + 0.13 * mom
+    assert rel(synth.from_ref(dims, lat.get_links(), 5, N), U2) < 1e-14
+    der = O.compute_derived(geo, prm, U2)
+    pd, D, F, Ui = lat.derived()
+    assert rel(synth.from_ref(dims, D, 1, N)[0], der.DmuUmu) < 1e-12
+
+
+@pytest.mark.parametrize("N", [2, 3])
+def test_action_parts(N):
+    dims = (4, 4, 4, 4)
+    lat, geo, prm, U = make(dims, N, lam=0.8, bmass=0.4, G=0.05, kappa_u1=0.3)
+    der = O.compute_derived(geo, prm, U)
+    mom = synth.links(dims, N, 0.3, 12) - np.eye(N)
+    lat.set_mom(synth.to_ref(dims, mom))
+    src = synth.tf_source(dims, N, 1)
+    sols = [synth.tf_source(dims, N, 2 + k) for k in range(4)]
+    amp = np.array([0.1, 0.2, 0.3, 0.4])
+    g, b, d, f, p = O.action_parts(geo, prm, U, der, mom, [src], [sols], amp, 0.37)
+    parts = lat.action([synth.to_ref(dims, src)], [[synth.to_ref(dims, s) for s in sols]],
+                       amp, 0.37)
+    for got, want in zip(parts, [g, b, d, f[0], p]):
+        assert abs(got - want) <= 1e-12 * abs(want)
+
+
+@pytest.mark.parametrize("N", [2, 3])
+def test_ranmom_and_gaussian_source(N):
+    dims = (4, 4, 2, 4)
+    lat = Lattice(dims, N, iseed=41)
+    geo = O.Geometry(dims, -1)
+    st = O.site_prn_lex(geo, 41)
+    lat.ranmom()
+    want = O.ranmom(st, N)
+    assert rel(synth.from_ref(dims, lat.get_mom(), 5, N), want) < 1e-12
+    R = lat.gaussian_tf()
+    assert rel(synth.from_ref(dims, R, 16, N), O.gaussian_tf(st, N)) < 1e-12
+
+
+def test_trajectory_matches_oracle():
+    dims, N = (4, 4, 4, 4), 2
+    kw = dict(lam=1.0, bmass=0.2, G=0.05, kappa_u1=0.0)
+    lat, geo, prm, U = make(dims, N, noise=0.1, seed=5, iseed=41, **kw)
+    tab = rhmc_table(15, 1)
+    r = RHMC(15, 1, nstep=2, nstep_gauge=2, traj_length=0.5, error_per_site=1e-6,
+             solver=SOLVER_FP64)
+    got = lat.update(r)
+    h = O.HMCState(geo=geo, prm=prm, U=U.copy(), mom=np.zeros_like(U),
+                   site_prn=O.site_prn_lex(geo, 41), node_prn=O.node_prn(geo, 41),
+                   rhmc=O.RHMC(**tab), Nroot=1, nsteps=(2, 2), traj_length=0.5,
+                   niter=5000, rsqmin=1e-12)
+    h.refresh()
+    want = O.update(h)
+    assert got["accept"] == want["accept"]
+    assert abs(got["start"] - want["start"]) < 1e-8 * abs(want["start"])
+    assert abs(got["delta_S"] - want["delta_S"]) < 1e-7
+    assert abs(got["iters"] - want["iters"]) <= 2 * 12
+    assert rel(synth.from_ref(dims, lat.get_links(), 5, N), h.U) < 1e-9
+
+
+def test_reversibility():
+    """Integrate, flip the momenta, integrate back: the links must return."""
+    dims, N = (4, 4, 4, 4), 2
+    lat, geo, prm, U = make(dims, N, noise=0.1, seed=6, lam=1.0, bmass=0.2, G=0.05)
+    r = RHMC(15, 1, nstep=3, nstep_gauge=2, traj_length=0.6, error_per_site=1e-10,
+             solver=SOLVER_FP64, no_metropolis=True)
+    U0 = lat.get_links()
+    mom0 = synth.to_ref(dims, synth.links(dims, N, 0.5, 21) - np.eye(N))
+    src = [synth.to_ref(dims, synth.tf_source(dims, N, 22, 0.3))]
+    a = lat.update_replay(r, mom0, src)
+    P1 = lat.get_mom()
+    b = lat.update_replay(r, -P1, src)
+    U2 = lat.get_links()
+    P2 = lat.get_mom()
+    assert np.abs(U2 - U0).max() < 1e-8
+    assert np.abs(P2 + mom0).max() < 1e-8
+    assert abs(a["delta_S"] + b["delta_S"]) < 1e-6
+
+
+@pytest.mark.parametrize("N", [2, 3])
+def test_mixed_solver_reaches_fp64_residual(N):
+    dims = (4, 4, 4, 8)
+    lat, geo, prm, U = make(dims, N, G=0.05)
+    der = O.compute_derived(geo, prm, U)
+    src = synth.tf_source(dims, N, 31)
+    shifts = np.array(rhmc_table(15, 1)["shift4"])
+    errormin = 1e-20
+    s64 = lat.tf(64)
+    s64.upload(synth.to_ref(dims, src))
+    psim = [lat.tf(64) for _ in shifts]
+    it, worst = lat.dev_congrad_multi(s64, psim, shifts, 20000, errormin, mixed=True)
+    b2 = O.magsq(src)
+    assert worst <= errormin * b2
+    for j, s in enumerate(shifts):
+        x = synth.from_ref(dims, psim[j].download(), 16, N)
+        res = O.DSq(geo, prm, U, der, x) + s * x - src
+        assert O.magsq(res) <= 1.5 * errormin * b2
+
+
+@pytest.mark.parametrize("N", [2, 3])
+def test_operator_variants_agree(N):
+    dims = (4, 4, 4, 8)
+    lat, geo, prm, U = make(dims, N, G=0.05)
+    der = O.compute_derived(geo, prm, U)
+    src = synth.tf_source(dims, N, 77)
+    want = O.DSq(geo, prm, U, der, src)
+    a, b = lat.tf(64), lat.tf(64)
+    a.upload(synth.to_ref(dims, src))
+    for v in range(3):
+        lat.fop_variant(64, v)
+        lat.dev_DSq(a, b)
+        assert rel(synth.from_ref(dims, b.download(), 16, N), want) < 1e-13, v
