@@ -1,0 +1,379 @@
+"""Benchmark of the RHMC fermion path on B200.
+
+Workload (the metric's configuration): 12^3 x 24 lattice, U(3) (NCOL = 3),
+lambda = 2, bmass = 0.3, G = 0.05, antiperiodic temporal BC; links seeded
+near the identity (noise 0.1, unthermalised); one multi-shift CG solve of
+the degree-15 RHMC system with Nroot = 2 (the 15 shift4 poles of
+setup_rhmc.c) on a complex-Gaussian Twist_Fermion source, to an FP64 true
+residual |r|^2 <= 1e-20 |src|^2 (error_per_site 1e-10).  One "step" is one
+such solve.  Inputs are resident in HBM when the timed region starts; the
+working set (~3 GB) is larger than L2, so no flush is needed.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--solver fp64|mixed]
+
+N > 1 runs one independent replica per GPU (torchrun, NCCL only for the
+barrier and the max-over-ranks time): "value" is the whole-job seconds per
+solve, max rank time / (K * N).  The reference arm times the reference's own
+CPU congrad_multi (oracle/_ref) on a bounded sample of the same solve.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+DIMS = (12, 12, 12, 24)
+NCOL = 3
+LAM, BMASS, G = 2.0, 0.3, 0.05
+LINK_NOISE, LINK_SEED, SRC_SEED = 0.1, 11, 12
+NORDER, NROOT = 15, 2
+ERRORMIN = 1e-20          # error_per_site 1e-10 squared (setup.c:356-359)
+MAXCG = 20000
+# Iterations the FP64 multi-shift solve of this seeded input takes (the
+# reference runs the identical recurrence); used to extrapolate the
+# reference arm's bounded sample to one full solve.
+REF_ITERS = 541
+REF_SAMPLE_ITERS = 2
+METRIC = "s/RHMC traj & CG solve time, 12^3x24 U(3): FP32+learned vs FP64 @1e-10 resid"
+WORKLOAD = ("12^3x24 U(3) multi-shift CG solve, Norder 15 / Nroot 2 shift4 poles, "
+            "FP64 true residual 1e-10 per site")
+
+
+def algorithmic_bytes_fop(V, N, w, doG=True):
+    """Bytes one fermion_op moves with perfect neighbour reuse:
+    V [(16 + 16 + 5) N^2 w + g (5 N^2 w + 20 w)], w = bytes per complex."""
+    return V * ((16 + 16 + 5) * N * N * w + (5 * N * N * w + 20 * w if doG else 0))
+
+
+def flops_fop(V, N):
+    """220 NCOL x NCOL complex products per site: 1760 N^3 flop per site."""
+    return 1760 * N ** 3 * V
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 6:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx.append(float(parts[1]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[2:6]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+def reference_cpu_samples(nsamples: int, iters: int):
+    """Time nsamples runs of `iters` iterations of the reference's
+    congrad_multi on the bench workload, each from the zero initial guess
+    (runs in this process; call through run_in_fresh_process)."""
+    from oracle.ref_ctypes import RefLattice
+    from susy_b200 import synth
+    from susy_b200.rhmc_tables import rhmc
+    ref = RefLattice(NCOL, dims=DIMS, pbc=-1, lam=LAM, bmass=BMASS, G=G, Nroot=NROOT,
+                     Norder=NORDER)
+    ref.set_links(synth.to_ref(DIMS, synth.links(DIMS, NCOL, LINK_NOISE, LINK_SEED)))
+    ref.compute_all()
+    src = synth.to_ref(DIMS, synth.tf_source(DIMS, NCOL, SRC_SEED))
+    shifts = np.array(rhmc(NORDER, NROOT)["shift4"])
+    out = []
+    for _ in range(nsamples):
+        t0 = time.perf_counter()
+        _, it, _ = ref.congrad_multi(src, shifts, iters, ERRORMIN)
+        out.append((time.perf_counter() - t0, it))
+    return out
+
+
+def port_cpu_samples(nsamples: int, iters: int):
+    """Same samples with the numpy restatement (when oracle/_ref is absent)."""
+    from oracle import susy_np as O
+    from susy_b200 import synth
+    from susy_b200.rhmc_tables import rhmc
+    geo = O.Geometry(DIMS, -1)
+    prm = O.Params(lam=LAM, bmass=BMASS, G=G, N=NCOL)
+    U = synth.links(DIMS, NCOL, LINK_NOISE, LINK_SEED)
+    der = O.compute_derived(geo, prm, U)
+    src = synth.tf_source(DIMS, NCOL, SRC_SEED)
+    shifts = np.array(rhmc(NORDER, NROOT)["shift4"])
+    out = []
+    for _ in range(nsamples):
+        t0 = time.perf_counter()
+        _, it, _ = O.congrad_multi(geo, prm, U, der, src, shifts, iters, ERRORMIN)
+        out.append((time.perf_counter() - t0, it))
+    return out
+
+
+def cpu_samples(nsamples=1, iters=REF_SAMPLE_ITERS):
+    """[(s/solve extrapolated, ...)] and the cpu_baseline description."""
+    from oracle.ref_ctypes import available, run_in_fresh_process
+    if available(NCOL):
+        res = run_in_fresh_process(reference_cpu_samples, nsamples, iters)
+        kind = "reference"
+    else:
+        res = run_in_fresh_process(port_cpu_samples, nsamples, iters)
+        kind = "port"
+    vals = [dt / max(it, 1) * REF_ITERS for dt, it in res]
+    per_iter = res[-1][0] / max(res[-1][1], 1)
+    desc = {"value": vals[-1], "unit": "s/solve", "cores": 1, "kind": kind,
+            "sample": "%d of the %d iterations of the full solve timed on one host core "
+                      "(%.3f s/iteration; the first iterations carry all 15 shifts), "
+                      "extrapolated to %d" % (res[-1][1], REF_ITERS, per_iter, REF_ITERS)}
+    return vals, desc
+
+
+def cpu_baseline(iters=REF_SAMPLE_ITERS):
+    return cpu_samples(1, iters)[1]
+
+
+# ---------------------------------------------------------------------------
+def run_reference_arm(args, rank, world):
+    if rank != 0:
+        return None
+    vals, base = cpu_samples(args.warmup + args.steps, REF_SAMPLE_ITERS)
+    v = statistics.mean(vals[args.warmup:])
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "s/solve",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": v * 1e3, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "lattice": "12x12x12x24", "ncol": NCOL,
+                       "norder": NORDER, "nroot": NROOT, "parallelism": "replicas"},
+            "cpu_baseline": {"value": v, "unit": "s/solve", "cores": base["cores"],
+                             "kind": base["kind"], "sample": base["sample"]},
+            "e2e": {"value": v, "unit": "s/solve", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return line
+
+
+def run_ours(args, rank, world, device):
+    import torch
+    import torch.distributed as dist
+    from susy_b200 import Lattice, synth
+    from susy_b200.lattice import launch_count
+    from susy_b200.replicas import max_over_ranks, rank_seed, seconds_per_solve
+    from susy_b200.rhmc_tables import rhmc
+
+    torch.cuda.set_device(device)
+    lat = Lattice(DIMS, NCOL, pbc=-1, lam=LAM, bmass=BMASS, G=G, device=device)
+    st = torch.cuda.Stream(device=device)
+    lat.set_stream(st.cuda_stream)
+    links = synth.links(DIMS, NCOL, LINK_NOISE, rank_seed(LINK_SEED, rank))
+    lat.set_links(synth.to_ref(DIMS, links))
+    src_host = synth.to_ref(DIMS, synth.tf_source(DIMS, NCOL, rank_seed(SRC_SEED, rank)))
+    shifts = np.array(rhmc(NORDER, NROOT)["shift4"])
+    src = lat.tf(64)
+    src.upload(src_host)
+    psim = [lat.tf(64) for _ in shifts]
+    lat.autotune()
+    mixed = args.solver == "mixed"
+
+    def solve():
+        return lat.dev_congrad_multi(src, psim, shifts, MAXCG, ERRORMIN, mixed=mixed)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    iters = []
+    for _ in range(args.warmup):
+        iters.append(solve()[0])
+    lat.sync()
+    barrier()
+    torch.cuda.synchronize(device)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    n0 = launch_count()
+    with ClockSampler(device) as clk:
+        e0.record(st)
+        for _ in range(args.steps):
+            it, rsq = solve()
+            iters.append(it)
+        e1.record(st)
+        e1.synchronize()
+    launches = launch_count() - n0
+    barrier()
+    torch.cuda.synchronize(device)
+    ms_max = max_over_ranks(e0.elapsed_time(e1))
+
+    # Dominant kernel: the fermion operator inside DSq, timed live on the
+    # launching stream after the timed region.
+    a = lat.tf(64)
+    b = lat.tf(64)
+    a.upload(src_host)
+    lat.dev_DSq(a, b)
+    reps = 10
+    f0 = torch.cuda.Event(enable_timing=True)
+    f1 = torch.cuda.Event(enable_timing=True)
+    f0.record(st)
+    for _ in range(reps):
+        lat.dev_DSq(a, b)
+    f1.record(st)
+    f1.synchronize()
+    fop_ms = f0.elapsed_time(f1) / (2 * reps)
+    V = lat.V
+    algo = algorithmic_bytes_fop(V, NCOL, 16)
+    achieved = algo / (fop_ms * 1e-3) / 1e9
+    peak, peak_kind = measured_peaks()
+    traffic = None
+    try:
+        with open(os.path.join(ROOT, "profiles", "fermion_op_12x12x12x24_u3.json")) as f:
+            traffic = json.load(f).get("dram_bytes_per_launch")
+    except Exception:
+        pass
+
+    # End to end through the public host API: source H2D, every solution D2H
+    e2e_ms = None
+    h2d = d2h = 0
+    if not args.no_e2e:
+        import torch as _t
+        host_src = _t.empty(lat.tf_doubles, dtype=_t.float64, pin_memory=True).numpy()
+        host_src[:] = src_host
+        outs = [_t.empty(lat.tf_doubles, dtype=_t.float64, pin_memory=True).numpy()
+                for _ in shifts]
+        lat.congrad_multi(host_src, outs, shifts, MAXCG, ERRORMIN)
+        barrier()
+        g0 = _t.cuda.Event(enable_timing=True)
+        g1 = _t.cuda.Event(enable_timing=True)
+        g0.record(st)
+        for _ in range(args.steps):
+            lat.congrad_multi(host_src, outs, shifts, MAXCG, ERRORMIN)
+        g1.record(st)
+        g1.synchronize()
+        e2e_ms = max_over_ranks(g0.elapsed_time(g1))
+        h2d = host_src.nbytes
+        d2h = sum(o.nbytes for o in outs)
+
+    if rank != 0:
+        return None
+    value = seconds_per_solve(ms_max, args.steps, world)
+    line = {"metric": METRIC, "value": value, "unit": "s/solve", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if not mixed else "f32+f64",
+            "data": "synthetic",
+            "config": {"workload": WORKLOAD, "lattice": "12x12x12x24", "ncol": NCOL,
+                       "lambda": LAM, "bmass": BMASS, "G": G, "norder": NORDER,
+                       "nroot": NROOT, "solver": args.solver,
+                       "parallelism": "replicas" if world > 1 else "single",
+                       "l2": "working set ~3 GB > 126 MB L2; no flush",
+                       "iterations_per_solve": iters[-1],
+                       "fop_variant": lat.fop_variant(64)[0]},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak,
+                         "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": traffic, "kernel": "fermion_op (FP64, in DSq)",
+                         "algorithmic_bytes_per_launch": algo, "launch_ms": fop_ms,
+                         "fp64_tflops": flops_fop(V, NCOL) / (fop_ms * 1e-3) / 1e12},
+            "clocks": clk.summary(),
+            "gpu_launches": launches,
+            "e2e": {"value": seconds_per_solve(e2e_ms, args.steps, world) if e2e_ms else None,
+                    "unit": "s/solve", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h}}
+    if world == 1 and not args.no_cpu:
+        try:
+            line["cpu_baseline"] = cpu_baseline()
+        except Exception as e:  # the checker is optional: report why it is absent
+            line["cpu_baseline"] = {"value": None, "unavailable": str(e)[:200]}
+    print(json.dumps(line), flush=True)
+    return line
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--solver", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference_arm(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    try:
+        run_ours(args, rank, world, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -64,6 +64,9 @@ const char *susy_b200_error_string(int code);
 int susy_b200_set_stream(susy_b200_lattice *h, void *cuda_stream);
 int susy_b200_sync(susy_b200_lattice *h);
 int susy_b200_volume(const susy_b200_lattice *h);
+/* Number of kernels this library has launched in this process (all handles);
+ * no reference counterpart, used to account GPU work in benchmarks. */
+long long susy_b200_launch_count(void);
 
 /* ---- gauge field and momenta (site.link / site.mom, lattice.h:37-45) --- */
 /* Upload links and recompute every derived field, as readin() and

@@ -5,6 +5,7 @@
 #include <cstring>
 #include <cmath>
 #include <vector>
+#include <atomic>
 #include "../../include/susy_b200.h"
 #include "kernels.h"
 #include "lattice.h"
@@ -13,6 +14,9 @@
 using namespace susy;
 
 namespace susy {
+
+static std::atomic<long long> g_launches(0);
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
 static size_t mat_c(const susy_b200_lattice* h) { return (size_t)h->N * h->N; }
 
@@ -239,6 +243,8 @@ void susy_b200_destroy(susy_b200_lattice* h) {
   if (h->own_stream) cudaStreamDestroy(h->own_stream);
   delete h;
 }
+
+long long susy_b200_launch_count(void) { return g_launches.load(); }
 
 int susy_b200_last_error(const susy_b200_lattice* h) { return h ? h->err : SUSY_B200_EINVAL; }
 

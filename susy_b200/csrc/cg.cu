@@ -211,28 +211,28 @@ void ms_init(MsState* st, const void* src, int prec, long n, double* part, int m
              double errormin, cudaStream_t s) {
   const int nb = vec_blocks(n);
   if (prec == 64)
-    k_norm2<double2><<<nb, UT, 0, s>>>((const double2*)src, n, part);
+    count_launch(), k_norm2<double2><<<nb, UT, 0, s>>>((const double2*)src, n, part);
   else
-    k_norm2<float2><<<nb, UT, 0, s>>>((const float2*)src, n, part);
-  k_ms_init<<<1, ST, 0, s>>>(st, part, nb, maxcg, errormin);
+    count_launch(), k_norm2<float2><<<nb, UT, 0, s>>>((const float2*)src, n, part);
+  count_launch(), k_ms_init<<<1, ST, 0, s>>>(st, part, nb, maxcg, errormin);
 }
 
 void ms_scalars1(MsState* st, const double* part, int np, cudaStream_t s) {
-  k_ms_scalars1<<<1, ST, 0, s>>>(st, part, np);
+  count_launch(), k_ms_scalars1<<<1, ST, 0, s>>>(st, part, np);
 }
 
 void ms_scalars2(MsState* st, const double* part, int np, cudaStream_t s) {
-  k_ms_scalars2<<<1, ST, 0, s>>>(st, part, np);
+  count_launch(), k_ms_scalars2<<<1, ST, 0, s>>>(st, part, np);
 }
 
 void ms_update_a(MsState* st, const MsVecs& v, int prec, int prec_x, long n, double* part,
                  cudaStream_t s) {
   if (prec == 64)
-    k_ms_update_a<double2, double2><<<vec_blocks(n), UT, 0, s>>>(st, v, n, part);
+    count_launch(), k_ms_update_a<double2, double2><<<vec_blocks(n), UT, 0, s>>>(st, v, n, part);
   else if (prec_x == 64)
-    k_ms_update_a<float2, double2><<<vec_blocks(n), UT, 0, s>>>(st, v, n, part);
+    count_launch(), k_ms_update_a<float2, double2><<<vec_blocks(n), UT, 0, s>>>(st, v, n, part);
   else
-    k_ms_update_a<float2, float2><<<vec_blocks(n), UT, 0, s>>>(st, v, n, part);
+    count_launch(), k_ms_update_a<float2, float2><<<vec_blocks(n), UT, 0, s>>>(st, v, n, part);
 }
 
 // r64 = b - ax, r32 = (float) r64, partials of |r64|^2
@@ -273,31 +273,31 @@ __global__ void k_scale(long n, double s, double2* x) {
 
 int residual_partials(long n, const void* b, const void* ax, void* r64, void* r32, double* part,
                       cudaStream_t s) {
-  k_residual<<<vec_blocks(n), UT, 0, s>>>(n, (const double2*)b, (const double2*)ax,
+  count_launch(), k_residual<<<vec_blocks(n), UT, 0, s>>>(n, (const double2*)b, (const double2*)ax,
                                           (double2*)r64, (float2*)r32, part);
   return vec_blocks(n);
 }
 
 void add_low(long n, const void* e32, void* x64, cudaStream_t s) {
-  k_add_low<<<vec_blocks(n), UT, 0, s>>>(n, (const float2*)e32, (double2*)x64);
+  count_launch(), k_add_low<<<vec_blocks(n), UT, 0, s>>>(n, (const float2*)e32, (double2*)x64);
 }
 
 void scale_field(long n, double sc, void* x, cudaStream_t s) {
-  k_scale<<<vec_blocks(n), UT, 0, s>>>(n, sc, (double2*)x);
+  count_launch(), k_scale<<<vec_blocks(n), UT, 0, s>>>(n, sc, (double2*)x);
 }
 
 void ms_update_b(MsState* st, const MsVecs& v, int prec, long n, cudaStream_t s) {
   if (prec == 64)
-    k_ms_update_b<double2><<<vec_blocks(n), UT, 0, s>>>(st, v, n);
+    count_launch(), k_ms_update_b<double2><<<vec_blocks(n), UT, 0, s>>>(st, v, n);
   else
-    k_ms_update_b<float2><<<vec_blocks(n), UT, 0, s>>>(st, v, n);
+    count_launch(), k_ms_update_b<float2><<<vec_blocks(n), UT, 0, s>>>(st, v, n);
 }
 
 void norm2_partials(const void* x, int prec, long n, double* part, cudaStream_t s) {
   if (prec == 64)
-    k_norm2<double2><<<vec_blocks(n), UT, 0, s>>>((const double2*)x, n, part);
+    count_launch(), k_norm2<double2><<<vec_blocks(n), UT, 0, s>>>((const double2*)x, n, part);
   else
-    k_norm2<float2><<<vec_blocks(n), UT, 0, s>>>((const float2*)x, n, part);
+    count_launch(), k_norm2<float2><<<vec_blocks(n), UT, 0, s>>>((const float2*)x, n, part);
 }
 
 }  // namespace susy

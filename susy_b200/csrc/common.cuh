@@ -20,6 +20,10 @@
 
 namespace susy {
 
+// Host-side count of kernel launches made by this library (every launch
+// site is written as "count_launch(), kernel<<<...>>>(...)").
+void count_launch();
+
 constexpr int NUMLINK = 5;
 constexpr int NPLAQ = 10;
 constexpr int NTF = 16;

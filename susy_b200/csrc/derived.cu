@@ -161,32 +161,32 @@ static inline int nb(long n) { return (int)((n + DT - 1) / DT); }
 void compute_uinv(const Geo& g, int N, const void* U, void* det, void* Uinv, cudaStream_t st) {
   const long n = (long)g.V * NUMLINK;
   switch (N) {
-    case 2: k_det_inv<2><<<nb(n), DT, 0, st>>>(g, (const double2*)U, (double2*)det, (double2*)Uinv); break;
-    case 3: k_det_inv<3><<<nb(n), DT, 0, st>>>(g, (const double2*)U, (double2*)det, (double2*)Uinv); break;
-    case 4: k_det_inv<4><<<nb(n), DT, 0, st>>>(g, (const double2*)U, (double2*)det, (double2*)Uinv); break;
+    case 2: count_launch(), k_det_inv<2><<<nb(n), DT, 0, st>>>(g, (const double2*)U, (double2*)det, (double2*)Uinv); break;
+    case 3: count_launch(), k_det_inv<3><<<nb(n), DT, 0, st>>>(g, (const double2*)U, (double2*)det, (double2*)Uinv); break;
+    case 4: count_launch(), k_det_inv<4><<<nb(n), DT, 0, st>>>(g, (const double2*)U, (double2*)det, (double2*)Uinv); break;
   }
 }
 
 void compute_plaqdet(const Geo& g, const void* det, void* pd, void* zw, cudaStream_t st) {
-  k_plaqdet<<<nb(g.V), DT, 0, st>>>(g, (const double2*)det, (double2*)pd, (double2*)zw);
+  count_launch(), k_plaqdet<<<nb(g.V), DT, 0, st>>>(g, (const double2*)det, (double2*)pd, (double2*)zw);
 }
 
 void compute_dmuumu(const Geo& g, int N, const void* U, const void* pd, double G, void* D,
                     cudaStream_t st) {
   const int doG = G > 1e-8;
   switch (N) {
-    case 2: k_dmuumu<2><<<nb(g.V), DT, 0, st>>>(g, (const double2*)U, (const double2*)pd, G, doG, (double2*)D); break;
-    case 3: k_dmuumu<3><<<nb(g.V), DT, 0, st>>>(g, (const double2*)U, (const double2*)pd, G, doG, (double2*)D); break;
-    case 4: k_dmuumu<4><<<nb(g.V), DT, 0, st>>>(g, (const double2*)U, (const double2*)pd, G, doG, (double2*)D); break;
+    case 2: count_launch(), k_dmuumu<2><<<nb(g.V), DT, 0, st>>>(g, (const double2*)U, (const double2*)pd, G, doG, (double2*)D); break;
+    case 3: count_launch(), k_dmuumu<3><<<nb(g.V), DT, 0, st>>>(g, (const double2*)U, (const double2*)pd, G, doG, (double2*)D); break;
+    case 4: count_launch(), k_dmuumu<4><<<nb(g.V), DT, 0, st>>>(g, (const double2*)U, (const double2*)pd, G, doG, (double2*)D); break;
   }
 }
 
 void compute_fmunu(const Geo& g, int N, const void* U, void* F, cudaStream_t st) {
   const long n = (long)g.V * NPLAQ;
   switch (N) {
-    case 2: k_fmunu<2><<<nb(n), DT, 0, st>>>(g, (const double2*)U, (double2*)F); break;
-    case 3: k_fmunu<3><<<nb(n), DT, 0, st>>>(g, (const double2*)U, (double2*)F); break;
-    case 4: k_fmunu<4><<<nb(n), DT, 0, st>>>(g, (const double2*)U, (double2*)F); break;
+    case 2: count_launch(), k_fmunu<2><<<nb(n), DT, 0, st>>>(g, (const double2*)U, (double2*)F); break;
+    case 3: count_launch(), k_fmunu<3><<<nb(n), DT, 0, st>>>(g, (const double2*)U, (double2*)F); break;
+    case 4: count_launch(), k_fmunu<4><<<nb(n), DT, 0, st>>>(g, (const double2*)U, (double2*)F); break;
   }
 }
 

@@ -194,8 +194,9 @@ template <int N, typename R, int SIGN, int MINB>
 __global__ void __launch_bounds__(FOP_THREADS, MINB)
 fermion_op_kernel(FopArgs<R> a) {
   if (a.skip && *a.skip) return;
-  const int comp = blockIdx.x % NTF;
-  const int s = (blockIdx.x / NTF) * FOP_THREADS + threadIdx.x;
+  const int comp = a.comp_major ? blockIdx.x / a.nsb : blockIdx.x % NTF;
+  const int sb = a.comp_major ? blockIdx.x % a.nsb : blockIdx.x / NTF;
+  const int s = sb * FOP_THREADS + threadIdx.x;
   const bool live = s < a.g.V;
   double part = 0.0;
   if (live) {
@@ -240,12 +241,13 @@ fermion_op_kernel(FopArgs<R> a) {
 }
 
 template <int N, typename R, int MINB>
-static int launch_fop(const FopArgs<R>& a, int sign, cudaStream_t st) {
-  const int nblk = ((a.g.V + FOP_THREADS - 1) / FOP_THREADS) * NTF;
+static int launch_fop(FopArgs<R> a, int sign, cudaStream_t st) {
+  a.nsb = (a.g.V + FOP_THREADS - 1) / FOP_THREADS;
+  const int nblk = a.nsb * NTF;
   if (sign > 0)
-    fermion_op_kernel<N, R, 1, MINB><<<nblk, FOP_THREADS, 0, st>>>(a);
+    count_launch(), fermion_op_kernel<N, R, 1, MINB><<<nblk, FOP_THREADS, 0, st>>>(a);
   else
-    fermion_op_kernel<N, R, -1, MINB><<<nblk, FOP_THREADS, 0, st>>>(a);
+    count_launch(), fermion_op_kernel<N, R, -1, MINB><<<nblk, FOP_THREADS, 0, st>>>(a);
   return nblk;
 }
 
@@ -272,13 +274,10 @@ int fermion_op(const Geo& g, int N, const void* U, const void* Uinv, const void*
   a.dot = dot;
   a.skip = skip;
   if (variant == FOP_ROWS) return fermion_op_rows<R>(a, N, sign, st);
+  a.comp_major = variant == FOP_MAT_CM;
   switch (N) {
-    case 2:
-      return variant == FOP_MAT_OCC ? launch_fop<2, R, 3>(a, sign, st)
-                                    : launch_fop<2, R, 1>(a, sign, st);
-    case 3:
-      return variant == FOP_MAT_OCC ? launch_fop<3, R, 2>(a, sign, st)
-                                    : launch_fop<3, R, 1>(a, sign, st);
+    case 2: return launch_fop<2, R, 1>(a, sign, st);
+    case 3: return launch_fop<3, R, 1>(a, sign, st);
     default: return launch_fop<4, R, 1>(a, sign, st);
   }
 }

@@ -218,11 +218,11 @@ __global__ void __launch_bounds__(RowShape<N>::NT)
 fermion_op_rows_kernel(FopArgs<R> a) {
   if (a.skip && *a.skip) return;
   typedef RowShape<N> SH;
-  const int comp = blockIdx.x % NTF;
+  const int comp = blockIdx.x / a.nsb;   // component-major block order
   const int lane = threadIdx.x & 31;
   const int i = (threadIdx.x >> 5) % N;
   const int grp = threadIdx.x / (32 * N);
-  const int s = (blockIdx.x / NTF) * SH::SB + grp * 32 + lane;
+  const int s = (blockIdx.x % a.nsb) * SH::SB + grp * 32 + lane;
   double part = 0.0;
   if (s < a.g.V) {
     const Site c = site_of(a.g, s);
@@ -267,13 +267,14 @@ fermion_op_rows_kernel(FopArgs<R> a) {
 }
 
 template <int N, typename R>
-static int launch_rows(const FopArgs<R>& a, int sign, cudaStream_t st) {
+static int launch_rows(FopArgs<R> a, int sign, cudaStream_t st) {
   typedef RowShape<N> SH;
-  const int nblk = ((a.g.V + SH::SB - 1) / SH::SB) * NTF;
+  a.nsb = (a.g.V + SH::SB - 1) / SH::SB;
+  const int nblk = a.nsb * NTF;
   if (sign > 0)
-    fermion_op_rows_kernel<N, R, 1><<<nblk, SH::NT, 0, st>>>(a);
+    count_launch(), fermion_op_rows_kernel<N, R, 1><<<nblk, SH::NT, 0, st>>>(a);
   else
-    fermion_op_rows_kernel<N, R, -1><<<nblk, SH::NT, 0, st>>>(a);
+    count_launch(), fermion_op_rows_kernel<N, R, -1><<<nblk, SH::NT, 0, st>>>(a);
   return nblk;
 }
 

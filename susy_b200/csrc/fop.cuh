@@ -19,6 +19,8 @@ struct FopArgs {
   R addc;
   double* dot;
   const int* skip;  // device flag: nonzero = do nothing (finished solves)
+  int comp_major;   // block order: 1 = all blocks of one output component together
+  int nsb;          // site blocks per component
 };
 
 constexpr int FOP_THREADS = 128;

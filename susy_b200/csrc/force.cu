@@ -468,20 +468,20 @@ void fermion_force_pole(const Geo& g, int N, const void* U, const void* Uinv, co
   a.doG = G > 1e-8;
   const int nb = force_blocks(g);
   switch (N) {
-    case 2: k_fermion_force<2><<<nb, FT, 0, st>>>(a); break;
-    case 3: k_fermion_force<3><<<nb, FT, 0, st>>>(a); break;
-    case 4: k_fermion_force<4><<<nb, FT, 0, st>>>(a); break;
+    case 2: count_launch(), k_fermion_force<2><<<nb, FT, 0, st>>>(a); break;
+    case 3: count_launch(), k_fermion_force<3><<<nb, FT, 0, st>>>(a); break;
+    case 4: count_launch(), k_fermion_force<4><<<nb, FT, 0, st>>>(a); break;
   }
 }
 
 int mom_sub(long n, const void* force, void* mom, double eps, double* part, cudaStream_t st) {
   const int nb = nbk(n, 256);
-  k_mom_sub<<<nb, 256, 0, st>>>(n, (const double2*)force, (double2*)mom, eps, part);
+  count_launch(), k_mom_sub<<<nb, 256, 0, st>>>(n, (const double2*)force, (double2*)mom, eps, part);
   return nb;
 }
 
 void axpy_field(long n, double s, const void* x, void* y, cudaStream_t st) {
-  k_axpy<<<nbk(n, 256), 256, 0, st>>>(n, s, (const double2*)x, (double2*)y);
+  count_launch(), k_axpy<<<nbk(n, 256), 256, 0, st>>>(n, s, (const double2*)x, (double2*)y);
 }
 
 int gauge_force(const Geo& g, int N, const void* U, const void* Uinv, const void* pd,
@@ -508,9 +508,9 @@ int gauge_force(const Geo& g, int N, const void* U, const void* Uinv, const void
   a.part = part;
   a.nblk = force_blocks(g);
   switch (N) {
-    case 2: k_gauge_force<2><<<a.nblk, FT, 0, st>>>(a); break;
-    case 3: k_gauge_force<3><<<a.nblk, FT, 0, st>>>(a); break;
-    case 4: k_gauge_force<4><<<a.nblk, FT, 0, st>>>(a); break;
+    case 2: count_launch(), k_gauge_force<2><<<a.nblk, FT, 0, st>>>(a); break;
+    case 3: count_launch(), k_gauge_force<3><<<a.nblk, FT, 0, st>>>(a); break;
+    case 4: count_launch(), k_gauge_force<4><<<a.nblk, FT, 0, st>>>(a); break;
   }
   return a.nblk;
 }
@@ -519,9 +519,9 @@ int action_partials(const Geo& g, int N, const void* U, const void* D, const voi
                     const void* pd, const void* mom, double* part, cudaStream_t st) {
   const int nb = site_blocks(g);
   switch (N) {
-    case 2: k_action<2><<<nb, FT, 0, st>>>(g, (const double2*)U, (const double2*)D, (const double2*)F, (const double2*)pd, (const double2*)mom, part, nb); break;
-    case 3: k_action<3><<<nb, FT, 0, st>>>(g, (const double2*)U, (const double2*)D, (const double2*)F, (const double2*)pd, (const double2*)mom, part, nb); break;
-    case 4: k_action<4><<<nb, FT, 0, st>>>(g, (const double2*)U, (const double2*)D, (const double2*)F, (const double2*)pd, (const double2*)mom, part, nb); break;
+    case 2: count_launch(), k_action<2><<<nb, FT, 0, st>>>(g, (const double2*)U, (const double2*)D, (const double2*)F, (const double2*)pd, (const double2*)mom, part, nb); break;
+    case 3: count_launch(), k_action<3><<<nb, FT, 0, st>>>(g, (const double2*)U, (const double2*)D, (const double2*)F, (const double2*)pd, (const double2*)mom, part, nb); break;
+    case 4: count_launch(), k_action<4><<<nb, FT, 0, st>>>(g, (const double2*)U, (const double2*)D, (const double2*)F, (const double2*)pd, (const double2*)mom, part, nb); break;
   }
   return nb;
 }
@@ -529,7 +529,7 @@ int action_partials(const Geo& g, int N, const void* U, const void* D, const voi
 int fermion_action_partials(long n, const void* src, int nsol, const void* const* sol_dev_array,
                             const double* amp_dev, double ampdeg, double* part, cudaStream_t st) {
   const int nb = nbk(n, 256);
-  k_fermion_action<<<nb, 256, 0, st>>>(n, (const double2*)src, nsol,
+  count_launch(), k_fermion_action<<<nb, 256, 0, st>>>(n, (const double2*)src, nsol,
                                         (const double2* const*)sol_dev_array, amp_dev, ampdeg,
                                         part);
   return nb;

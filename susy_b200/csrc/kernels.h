@@ -27,9 +27,10 @@ struct MsVecs {
 };
 
 // fermion_op.cu, fermion_op_rows.cu
-// Kernel variants: matrix per thread, the same with a register cap for
-// occupancy, and one matrix row per thread.
-enum { FOP_MAT = 0, FOP_MAT_OCC = 1, FOP_ROWS = 2, FOP_NVARIANTS = 3 };
+// Kernel variants: matrix per thread with the 16 output components
+// interleaved block by block, the same with component-major block order,
+// and one matrix row per thread (component-major).
+enum { FOP_MAT = 0, FOP_MAT_CM = 1, FOP_ROWS = 2, FOP_NVARIANTS = 3 };
 template <typename R>
 int fermion_op(const Geo& g, int N, const void* U, const void* Uinv, const void* pd,
                 const void* src, void* dst, int sign, double G, const void* add, double addc,

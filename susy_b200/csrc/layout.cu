@@ -61,25 +61,25 @@ static inline int nbl(long n) { return (int)((n + LT - 1) / LT); }
 void aos_to_soa(const Geo& g, int K, int N, const void* aos, void* soa, int prec, cudaStream_t st) {
   const long n = (long)K * N * N * g.V;
   if (prec == 64)
-    k_aos_to_soa<double2><<<nbl(n), LT, 0, st>>>(g, K, N * N, (const double2*)aos, (double2*)soa);
+    count_launch(), k_aos_to_soa<double2><<<nbl(n), LT, 0, st>>>(g, K, N * N, (const double2*)aos, (double2*)soa);
   else
-    k_aos_to_soa<float2><<<nbl(n), LT, 0, st>>>(g, K, N * N, (const double2*)aos, (float2*)soa);
+    count_launch(), k_aos_to_soa<float2><<<nbl(n), LT, 0, st>>>(g, K, N * N, (const double2*)aos, (float2*)soa);
 }
 
 void soa_to_aos(const Geo& g, int K, int N, const void* soa, void* aos, int prec, cudaStream_t st) {
   const long n = (long)K * N * N * g.V;
   if (prec == 64)
-    k_soa_to_aos<double2><<<nbl(n), LT, 0, st>>>(g, K, N * N, (const double2*)soa, (double2*)aos);
+    count_launch(), k_soa_to_aos<double2><<<nbl(n), LT, 0, st>>>(g, K, N * N, (const double2*)soa, (double2*)aos);
   else
-    k_soa_to_aos<float2><<<nbl(n), LT, 0, st>>>(g, K, N * N, (const float2*)soa, (double2*)aos);
+    count_launch(), k_soa_to_aos<float2><<<nbl(n), LT, 0, st>>>(g, K, N * N, (const float2*)soa, (double2*)aos);
 }
 
 void convert_field(long ncomplex, const void* in, int prec_in, void* out, int prec_out,
                    cudaStream_t st) {
   if (prec_in == 64 && prec_out == 32)
-    k_convert<double2, float2><<<nbl(ncomplex), LT, 0, st>>>(ncomplex, (const double2*)in, (float2*)out);
+    count_launch(), k_convert<double2, float2><<<nbl(ncomplex), LT, 0, st>>>(ncomplex, (const double2*)in, (float2*)out);
   else if (prec_in == 32 && prec_out == 64)
-    k_convert<float2, double2><<<nbl(ncomplex), LT, 0, st>>>(ncomplex, (const float2*)in, (double2*)out);
+    count_launch(), k_convert<float2, double2><<<nbl(ncomplex), LT, 0, st>>>(ncomplex, (const float2*)in, (double2*)out);
   else if (prec_in == 64)
     cudaMemcpyAsync(out, in, ncomplex * sizeof(double2), cudaMemcpyDeviceToDevice, st);
   else

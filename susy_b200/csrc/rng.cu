@@ -142,16 +142,16 @@ __global__ void k_gauss_fill(Geo g, uint32_t* st, const double2* gen, int K, int
 }
 
 void init_prn(const Geo& g, int seed, void* st, cudaStream_t s) {
-  k_init_prn<<<(g.V + 127) / 128, 128, 0, s>>>(g, seed, (uint32_t*)st);
+  count_launch(), k_init_prn<<<(g.V + 127) / 128, 128, 0, s>>>(g, seed, (uint32_t*)st);
 }
 
 void gauss_fill(const Geo& g, int N, void* st, const void* gen, int K, int gen_outer, void* out,
                 int* bad, cudaStream_t s) {
   const int nb = (g.V + 127) / 128;
   switch (N) {
-    case 2: k_gauss_fill<2><<<nb, 128, 0, s>>>(g, (uint32_t*)st, (const double2*)gen, K, gen_outer, (double2*)out, bad); break;
-    case 3: k_gauss_fill<3><<<nb, 128, 0, s>>>(g, (uint32_t*)st, (const double2*)gen, K, gen_outer, (double2*)out, bad); break;
-    case 4: k_gauss_fill<4><<<nb, 128, 0, s>>>(g, (uint32_t*)st, (const double2*)gen, K, gen_outer, (double2*)out, bad); break;
+    case 2: count_launch(), k_gauss_fill<2><<<nb, 128, 0, s>>>(g, (uint32_t*)st, (const double2*)gen, K, gen_outer, (double2*)out, bad); break;
+    case 3: count_launch(), k_gauss_fill<3><<<nb, 128, 0, s>>>(g, (uint32_t*)st, (const double2*)gen, K, gen_outer, (double2*)out, bad); break;
+    case 4: count_launch(), k_gauss_fill<4><<<nb, 128, 0, s>>>(g, (uint32_t*)st, (const double2*)gen, K, gen_outer, (double2*)out, bad); break;
   }
 }
 

@@ -102,6 +102,8 @@ def load_library(path: str = LIB_PATH):
     L.susy_b200_set_stream.argtypes = [_vp, _vp]
     L.susy_b200_sync.argtypes = [_vp]
     L.susy_b200_volume.argtypes = [_vp]
+    L.susy_b200_launch_count.restype = C.c_longlong
+    L.susy_b200_launch_count.argtypes = []
     for name in ("set_links", "get_links", "set_mom", "get_mom"):
         getattr(L, "susy_b200_" + name).argtypes = [_vp, _dp, C.c_size_t]
     for name in ("compute_plaqdet", "compute_Uinv", "compute_DmuUmu", "compute_Fmunu"):
@@ -146,6 +148,11 @@ def load_library(path: str = LIB_PATH):
                                           _dp, C.POINTER(_dp)]
     _lib = L
     return L
+
+
+def launch_count() -> int:
+    """Kernels launched by libsusy_b200.so so far in this process."""
+    return int(load_library().susy_b200_launch_count())
 
 
 def _ptr(a: np.ndarray):

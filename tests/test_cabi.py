@@ -1,0 +1,68 @@
+"""The C-ABI library loads and exports every entry point include/*.h declares.
+
+CPU only: no compute call is made (there is no GPU here); creating a lattice
+without a GPU must fail cleanly with NULL, never crash.
+"""
+import ctypes as C
+import glob
+import os
+import re
+
+import pytest
+
+from susy_b200 import lattice as L
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_functions():
+    names = set()
+    for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
+        txt = open(h).read()
+        txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+        for m in re.finditer(r"\b(susy_b200_[A-Za-z0-9_]+)\s*\(", txt):
+            names.add(m.group(1))
+    return sorted(names)
+
+
+def test_header_declares_entry_points():
+    names = declared_functions()
+    for must in ("susy_b200_fermion_op", "susy_b200_DSq", "susy_b200_congrad_multi",
+                 "susy_b200_fermion_force", "susy_b200_gauge_force", "susy_b200_det_force",
+                 "susy_b200_update_u", "susy_b200_update", "susy_b200_action",
+                 "susy_b200_compute_plaqdet", "susy_b200_compute_Uinv",
+                 "susy_b200_compute_DmuUmu", "susy_b200_compute_Fmunu",
+                 "susy_b200_ranmom", "susy_b200_grsource"):
+        assert must in names
+
+
+def test_library_exports_every_declared_symbol():
+    lib = L.load_library()
+    missing = [n for n in declared_functions() if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_error_strings_and_null_handles():
+    lib = L.load_library()
+    assert lib.susy_b200_error_string(0) == b"ok"
+    assert lib.susy_b200_error_string(-1) == b"invalid argument"
+    assert lib.susy_b200_last_error(None) == -1
+    assert lib.susy_b200_fermion_op(None, None, None, 1) == -1
+
+
+def test_create_rejects_bad_geometry_without_gpu_work():
+    lib = L.load_library()
+    p = L.Params(5, 4, 4, 4, 2, -1, 0.5, 0, 0, 0, 0, 41, 0)   # odd nx
+    assert not lib.susy_b200_create(C.byref(p))
+    p = L.Params(4, 4, 4, 4, 7, -1, 0.5, 0, 0, 0, 0, 41, 0)   # NCOL 7
+    assert not lib.susy_b200_create(C.byref(p))
+    p = L.Params(4, 4, 4, 4, 2, 0, 0.5, 0, 0, 0, 0, 41, 0)    # PBC 0
+    assert not lib.susy_b200_create(C.byref(p))
+
+
+def test_lattice_without_gpu_raises_loudly():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    with pytest.raises(L.SusyError):
+        L.Lattice((4, 4, 4, 4), 2)

@@ -1,0 +1,119 @@
+"""The CUDA path against vectors and regression output of the reference itself.
+
+ops_U{2,3}.npz hold the UNMODIFIED reference's outputs on seeded inputs
+(tests/golden/make_golden.py); hmc_U{2,3}.json are the reference's own
+regression goldens testsuite/scalar/hmc.U{2,3}.ref (3 trajectories each,
+printed to 8-12 significant digits), run here from the same starting
+configuration and parameters through the C ABI.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from susy_b200 import Lattice, RHMC, SOLVER_FP64, SOLVER_MIXED
+from susy_b200 import synth
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def rel(a, b):
+    return float(np.abs(a - b).max() / np.abs(b).max())
+
+
+def lattice_from_ops(d):
+    dims = tuple(int(x) for x in d["dims"])
+    N = int(d["N"])
+    lat = Lattice(dims, N, pbc=-1, lam=1.0, bmass=0.3, G=0.05, kappa_u1=0.4, iseed=41)
+    lat.set_links(np.ascontiguousarray(d["links"]))
+    return lat, dims, N
+
+
+@pytest.mark.parametrize("N", [2, 3])
+def test_cuda_matches_reference_vectors(N):
+    d = dict(np.load(os.path.join(GOLD, "ops_U%d.npz" % N)))
+    lat, dims, N = lattice_from_ops(d)
+    pd, D, F, Ui = lat.derived()
+    V = lat.V
+    m = np.tile(~np.eye(5, dtype=bool).reshape(-1), V)
+    pdr = d["plaqdet"].reshape(-1, 2)[m]
+    assert rel(pd.reshape(-1, 2)[m], pdr) < 1e-13
+    assert rel(D, d["DmuUmu"]) < 1e-13
+    assert rel(F, d["Fmunu"]) < 1e-13
+    assert rel(Ui, d["Uinv"]) < 1e-13
+    out = np.zeros(lat.tf_doubles)
+    lat.fermion_op(d["src"], out, 1)
+    assert rel(out, d["fop_plus"]) < 1e-13
+    lat.fermion_op(d["src"], out, -1)
+    assert rel(out, d["fop_minus"]) < 1e-13
+    lat.DSq(d["src"], out)
+    assert rel(out, d["DSq"]) < 1e-13
+    shifts = d["cg_shifts"]
+    psim = [np.zeros(lat.tf_doubles) for _ in shifts]
+    it, rsq = lat.congrad_multi(d["src"], psim, shifts, 5000, 1e-20)
+    assert abs(it - int(d["cg_iters"])) <= 1
+    for k, j in enumerate(d["cg_keep"]):
+        assert rel(psim[j], d["cg_psim"][k]) < 1e-9
+    lat.set_mom(np.zeros(lat.link_doubles))
+    fn = lat.fermion_force(0.11, None, [np.ascontiguousarray(s) for s in d["ff_sol"]],
+                           d["ff_amp"])
+    assert abs(fn - float(d["ff_norm"])) <= 1e-12 * abs(fn)
+    assert rel(lat.get_mom(), d["ff_mom"]) < 1e-12
+    lat.set_mom(np.ascontiguousarray(d["gf_mom0"]))
+    gn = lat.gauge_force(0.07)
+    assert abs(gn - float(d["gf_norm"])) <= 1e-12 * abs(gn)
+    assert rel(lat.get_mom(), d["gf_mom"]) < 1e-12
+    lat.set_mom(np.ascontiguousarray(d["gf_mom0"]))
+    full = [np.zeros(lat.tf_doubles) for _ in d["action_amp4"]]
+    lat.congrad_multi(d["src"], full, shifts, 5000, 1e-20)
+    parts = lat.action([d["src"]], [full], d["action_amp4"], float(d["action_ampdeg4"]))
+    for got, want in zip(parts, d["action_parts"]):
+        assert abs(got - want) <= 1e-9 * abs(want)
+    lat.ranmom()
+    assert rel(lat.get_mom(), d["ranmom"]) < 1e-13
+
+
+def run_hmc_ref(N, solver):
+    gold = json.load(open(os.path.join(GOLD, "hmc_U%d.json" % N)))
+    cfg = np.load(os.path.join(GOLD, "config_U%d_4444.npz" % N))
+    inp = gold["input"]
+    dims = tuple(int(x) for x in cfg["dims"])
+    lat = Lattice(dims, N, pbc=int(inp["PBC"]), lam=float(inp["lambda"]),
+                  bmass=float(inp["bmass"]), fmass=float(inp["fmass"]),
+                  kappa_u1=float(inp["kappa_u1"]), G=float(inp["G"]), iseed=int(inp["iseed"]))
+    lat.set_links(synth.to_ref(dims, cfg["links"].astype(np.complex128)))
+    r = RHMC(int(inp["Norder"]), int(inp["Nroot"]), nstep=int(inp["nstep"]),
+             nstep_gauge=int(inp["nstep_gauge"]), traj_length=float(inp["traj_length"]),
+             niter=int(inp["max_cg_iterations"]), error_per_site=float(inp["error_per_site"]),
+             solver=solver)
+    return gold, [lat.update(r) for _ in gold["trajectories"]]
+
+
+@pytest.mark.parametrize("N", [2, 3])
+def test_cuda_reproduces_hmc_regression_output(N):
+    gold, got = run_hmc_ref(N, SOLVER_FP64)
+    for g, t in zip(got, gold["trajectories"]):
+        for a, b in zip(g["start_parts"], t["start_action"][:5]):
+            assert abs(a - b) <= 5e-8 * abs(b)
+        for a, b in zip(g["end_parts"], t["end_action"][:5]):
+            assert abs(a - b) <= 5e-8 * abs(b)
+        assert g["accept"] == t["accept"]
+        assert abs(g["start"] - t["start_S"]) < 1e-6
+        assert abs(g["end"] - t["end_S"]) < 1e-6
+        assert abs(g["delta_S"] - t["delta_S"]) <= 1e-3 * max(abs(t["delta_S"]), 1e-3)
+        assert abs(g["iters"] - t["it_per_traj"]) <= 12
+        assert g["gnorm"] == pytest.approx(t["monitor"][0], rel=2e-3)
+        assert g["max_gf"] == pytest.approx(t["monitor"][1], rel=2e-3)
+        assert g["fnorm"][0] == pytest.approx(t["monitor"][2], rel=2e-3)
+        assert g["max_ff"][0] == pytest.approx(t["monitor"][3], rel=2e-3)
+
+
+def test_mixed_solver_keeps_the_accept_decisions():
+    """The mixed-precision solver reaches the same FP64 true-residual bound,
+    so the trajectories and accept/reject decisions stay those of the golden."""
+    gold, got = run_hmc_ref(2, SOLVER_MIXED)
+    for g, t in zip(got, gold["trajectories"]):
+        assert g["accept"] == t["accept"]
+        assert abs(g["delta_S"] - t["delta_S"]) <= 0.05

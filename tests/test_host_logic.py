@@ -1,0 +1,65 @@
+"""Host-side logic: layouts, gauge-file I/O, RHMC tables, replica plumbing."""
+import os
+
+import numpy as np
+import pytest
+
+from susy_b200 import synth
+from susy_b200.io_lat import read_gauge, write_gauge
+from susy_b200.rhmc_tables import TABLES, rhmc
+
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+@pytest.mark.parametrize("dims", [(4, 4, 4, 4), (2, 2, 2, 2), (12, 12, 12, 24), (4, 2, 6, 8)])
+def test_node_index_is_a_bijection_even_sites_first(dims):
+    ni = synth.node_index(dims)
+    V = int(np.prod(dims))
+    assert sorted(ni.tolist()) == list(range(V))
+    i = np.arange(V)
+    x, y = i % dims[0], (i // dims[0]) % dims[1]
+    z, t = (i // (dims[0] * dims[1])) % dims[2], i // (dims[0] * dims[1] * dims[2])
+    even = (x + y + z + t) % 2 == 0
+    assert ni[even].max() < V // 2 <= ni[~even].min()
+
+
+def test_ref_layout_roundtrip():
+    dims, N = (4, 2, 2, 4), 3
+    f = synth.tf_source(dims, N, 5)
+    assert np.array_equal(synth.from_ref(dims, synth.to_ref(dims, f), 16, N), f)
+
+
+def test_gauge_file_roundtrip(tmp_path):
+    dims, N = (4, 4, 2, 2), 3
+    U = synth.links(dims, N, 0.3, 7).astype(np.complex64).astype(np.complex128)
+    p = str(tmp_path / "cfg")
+    s29, s31 = write_gauge(p, dims, U, stamp="test")
+    d2, n2, U2, info = read_gauge(p)
+    assert d2 == dims and n2 == N and info["checksum_ok"]
+    assert (info["sum29"], info["sum31"]) == (s29, s31)
+    assert np.array_equal(U2, U)
+
+
+def test_reference_config_checksums_from_fixture():
+    cfg = np.load(os.path.join(GOLD, "config_U2_4444.npz"))
+    from susy_b200.io_lat import checksums
+    U = cfg["links"]
+    a = np.moveaxis(U, 0, 1)
+    words = np.stack([a.real, a.imag], -1).astype("<f4").reshape(-1).view("<u4")
+    # checksums of the reference's own config.U2.4444 (its .info file)
+    assert checksums(words) == (0x632f69a0, 0x0bb8becc)
+    assert (int(cfg["sum29"]), int(cfg["sum31"])) == (0x632f69a0, 0x0bb8becc)
+
+
+def test_rhmc_degree15_tables():
+    t1 = rhmc(15, 1)
+    assert len(t1["amp4"]) == 15 and t1["ampdeg4"] == pytest.approx(9.5797060554725838e-02)
+    assert t1["shift4"][0] == pytest.approx(3.1085594175442315e-08)
+    t2 = rhmc(15, 2)
+    assert all(np.diff(t2["shift4"]) > 0)
+    assert (15, 1) in TABLES and (15, 2) in TABLES
+
+
+def test_geometric_shifts():
+    s = synth.geometric_shifts(15, 1e-5, 1e3)
+    assert s[0] == pytest.approx(1e-5) and s[-1] == pytest.approx(1e3)
