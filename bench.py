@@ -44,7 +44,7 @@ MAXCG = 20000
 # Iterations the FP64 multi-shift solve of this seeded input takes (the
 # reference runs the identical recurrence); used to extrapolate the
 # reference arm's bounded sample to one full solve.
-REF_ITERS = 541
+REF_ITERS = 567
 REF_SAMPLE_ITERS = 2
 METRIC = "s/RHMC traj & CG solve time, 12^3x24 U(3): FP32+learned vs FP64 @1e-10 resid"
 WORKLOAD = ("12^3x24 U(3) multi-shift CG solve, Norder 15 / Nroot 2 shift4 poles, "

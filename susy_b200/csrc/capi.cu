@@ -89,9 +89,9 @@ static int launch_variant(susy_b200_lattice* h, const void* src, void* dst, int 
                           const void* add, double addc, double* dot, const int* skip, int v) {
   if (prec == 64)
     return fermion_op<double>(h->g, h->N, h->U, h->Uinv, h->pd, src, dst, sign, h->G, add, addc,
-                              dot, skip, v, h->stream);
+                              dot, skip, v, h->nbrtab, h->stream);
   return fermion_op<float>(h->g, h->N, h->U32, h->Uinv32, h->pd32, src, dst, sign, h->G, add,
-                           addc, dot, skip, v, h->stream);
+                           addc, dot, skip, v, h->nbrtab, h->stream);
 }
 
 // Project-written autotuner: time one D^dag D with every kernel variant on
@@ -186,6 +186,12 @@ susy_b200_lattice* susy_b200_create(const susy_b200_params* p) {
     return nullptr;
   }
   h->stream = h->own_stream;
+  if (upload_fop_terms(p->device, h->stream) != 0) {
+    cudaGetLastError();
+    cudaStreamDestroy(h->own_stream);
+    delete h;
+    return nullptr;
+  }
   const size_t m5 = field_bytes(h, 5, 64);
   h->U = dalloc(h, m5);
   h->mom = dalloc(h, m5);
@@ -201,6 +207,8 @@ susy_b200_lattice* susy_b200_create(const susy_b200_params* p) {
   h->pd32 = dalloc(h, 25 * h->g.S * sizeof(float2));
   h->stage = dalloc(h, (size_t)h->g.V * NTF * mat_c(h) * 2 * sizeof(double));
   h->ms = (MsState*)dalloc(h, sizeof(MsState));
+  h->nbrtab = (int*)dalloc(h, (size_t)fop_ndisp() * h->g.S * sizeof(int));
+  if (h->nbrtab) build_nbr_table(h->g, h->nbrtab, h->stream);
   if (h->err) {
     susy_b200_destroy(h);
     return nullptr;
@@ -226,7 +234,7 @@ void susy_b200_destroy(susy_b200_lattice* h) {
   cudaStreamSynchronize(h->stream);
   void* ptrs[] = {h->U, h->mom, h->Uinv, h->force, h->det, h->pd, h->zw, h->D, h->F,
                   h->U32, h->Uinv32, h->pd32, h->stage, h->ms, h->bigpart, h->gen, h->prn,
-                  h->rng_bad, h->ptrbuf};
+                  h->rng_bad, h->ptrbuf, h->nbrtab};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (int i = 0; i < SUSY_NSCRATCH; i++) {

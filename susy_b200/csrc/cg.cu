@@ -53,6 +53,9 @@ __global__ void k_ms_init(MsState* st, const double* partials, int np, int maxcg
       st->beta_i[j] = 0.0;
       st->converged[j] = 0;
       st->active_p[j] = 1;
+      st->pz[j] = 1.0;
+      st->pa[j] = 0.0;
+      st->pact[j] = 1;
     }
     st->skip = (st->rsq <= st->rsqstop || maxcg <= 0) ? 1 : 0;
     st->skip_b = 1;
@@ -111,6 +114,11 @@ __global__ void k_ms_scalars2(MsState* st, const double* partials, int np) {
     st->active_p[j] = !st->converged[j];
     if (st->converged[j]) continue;
     st->alpha[j] = a0 * st->zeta_ip1[j] * st->beta_i[j] / (st->zeta_i[j] * st->beta_i[0]);
+  }
+  for (int j = 0; j < st->nshift; j++) {
+    st->pz[j] = st->zeta_ip1[j];
+    st->pa[j] = st->alpha[j];
+    st->pact[j] = st->active_p[j];
   }
   st->rsq = rsqnew;
   for (int j = 1; j < st->nshift; j++) {
@@ -190,6 +198,74 @@ __global__ void __launch_bounds__(UT) k_ms_update_b(MsState* st, MsVecs v, long 
     p.y = sz[j] * r.y + sa[j] * p.y;
     *pp = p;
   }
+}
+
+// One pass per iteration over every live shift (congrad_multi.c:109-150 with
+// the p_j update of the previous iteration folded in):
+//   p_j = pz_j r + pa_j p_j  (deferred from the previous iteration, j >= 1)
+//   psi_j -= beta_j p_j      (j = 0 uses p0, updated by k_ms_update_p0)
+//   r += beta_0 mp;  partials of |r|^2
+// Each live shift costs 4 field streams (read p, psi; write p, psi); the
+// arithmetic per element is the same as the two-pass form.
+template <typename VT, typename XT>
+__global__ void __launch_bounds__(UT) k_ms_update_fused(MsState* st, MsVecs v, long n,
+                                                        double* part) {
+  __shared__ double sb[MS_MAXS], sz[MS_MAXS], sa[MS_MAXS];
+  __shared__ int sc[MS_MAXS], sp[MS_MAXS];
+  if (st->skip) return;
+  const int ns = st->nshift;
+  if (threadIdx.x < ns) {
+    const int j = threadIdx.x;
+    sb[j] = st->beta_i[j];
+    sc[j] = j == 0 ? 0 : st->converged[j];
+    sz[j] = st->pz[j];
+    sa[j] = st->pa[j];
+    sp[j] = j == 0 ? 0 : st->pact[j];
+  }
+  __syncthreads();
+  const long i = (long)blockIdx.x * UT + threadIdx.x;
+  double acc = 0.0;
+  if (i < n) {
+    VT rr = ((VT*)v.r)[i];
+#pragma unroll 1
+    for (int j = 0; j < ns; j++) {
+      if (sc[j]) continue;
+      VT* pq = (VT*)v.p[j] + i;
+      VT pj = *pq;
+      if (sp[j]) {
+        pj.x = sz[j] * rr.x + sa[j] * pj.x;
+        pj.y = sz[j] * rr.y + sa[j] * pj.y;
+        *pq = pj;
+      }
+      XT* pp = (XT*)v.psi[j] + i;
+      XT x = *pp;
+      x.x -= sb[j] * pj.x;
+      x.y -= sb[j] * pj.y;
+      *pp = x;
+    }
+    const VT m = ((const VT*)v.mp)[i];
+    rr.x += sb[0] * m.x;
+    rr.y += sb[0] * m.y;
+    ((VT*)v.r)[i] = rr;
+    acc = (double)rr.x * rr.x + (double)rr.y * rr.y;
+  }
+  acc = block_sum<UT>(acc);
+  if (threadIdx.x == 0) part[blockIdx.x] = acc;
+}
+
+// p0 = r + alpha_0 p0 (zeta_0 = 1), ahead of the next D^dag D p0
+template <typename VT>
+__global__ void __launch_bounds__(UT) k_ms_update_p0(MsState* st, MsVecs v, long n) {
+  if (st->skip_b) return;
+  const long i = (long)blockIdx.x * UT + threadIdx.x;
+  if (i >= n) return;
+  const double a0 = st->alpha[0];
+  const VT r = ((const VT*)v.r)[i];
+  VT* pp = (VT*)v.p[0] + i;
+  VT p = *pp;
+  p.x = r.x + a0 * p.x;
+  p.y = r.y + a0 * p.y;
+  *pp = p;
 }
 
 // |x|^2 partials over n complex entries
@@ -291,6 +367,23 @@ void ms_update_b(MsState* st, const MsVecs& v, int prec, long n, cudaStream_t s)
     count_launch(), k_ms_update_b<double2><<<vec_blocks(n), UT, 0, s>>>(st, v, n);
   else
     count_launch(), k_ms_update_b<float2><<<vec_blocks(n), UT, 0, s>>>(st, v, n);
+}
+
+void ms_update_fused(MsState* st, const MsVecs& v, int prec, int prec_x, long n, double* part,
+                     cudaStream_t s) {
+  if (prec == 64)
+    count_launch(), k_ms_update_fused<double2, double2><<<vec_blocks(n), UT, 0, s>>>(st, v, n, part);
+  else if (prec_x == 64)
+    count_launch(), k_ms_update_fused<float2, double2><<<vec_blocks(n), UT, 0, s>>>(st, v, n, part);
+  else
+    count_launch(), k_ms_update_fused<float2, float2><<<vec_blocks(n), UT, 0, s>>>(st, v, n, part);
+}
+
+void ms_update_p0(MsState* st, const MsVecs& v, int prec, long n, cudaStream_t s) {
+  if (prec == 64)
+    count_launch(), k_ms_update_p0<double2><<<vec_blocks(n), UT, 0, s>>>(st, v, n);
+  else
+    count_launch(), k_ms_update_p0<float2><<<vec_blocks(n), UT, 0, s>>>(st, v, n);
 }
 
 void norm2_partials(const void* x, int prec, long n, double* part, cudaStream_t s) {

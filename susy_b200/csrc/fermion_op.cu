@@ -258,7 +258,8 @@ int fop_partials(const Geo& g) { return ((g.V + 31) / 32) * NTF; }
 template <typename R>
 int fermion_op(const Geo& g, int N, const void* U, const void* Uinv, const void* pd,
                 const void* src, void* dst, int sign, double G, const void* add,
-                double addc, double* dot, const int* skip, int variant, cudaStream_t st) {
+                double addc, double* dot, const int* skip, int variant, const int* nbrtab,
+                cudaStream_t st) {
   typedef typename CT<R>::T T;
   FopArgs<R> a;
   a.g = g;
@@ -273,7 +274,10 @@ int fermion_op(const Geo& g, int N, const void* U, const void* Uinv, const void*
   a.addc = (R)addc;
   a.dot = dot;
   a.skip = skip;
+  a.nbrtab = nbrtab;
   if (variant == FOP_ROWS) return fermion_op_rows<R>(a, N, sign, st);
+  if (variant == FOP_COMPACT || variant == FOP_COMPACT_PF)
+    return fermion_op_compact<R>(a, N, sign, variant == FOP_COMPACT_PF, st);
   a.comp_major = variant == FOP_MAT_CM;
   switch (N) {
     case 2: return launch_fop<2, R, 1>(a, sign, st);
@@ -284,9 +288,9 @@ int fermion_op(const Geo& g, int N, const void* U, const void* Uinv, const void*
 
 template int fermion_op<double>(const Geo&, int, const void*, const void*, const void*,
                                  const void*, void*, int, double, const void*, double,
-                                 double*, const int*, int, cudaStream_t);
+                                 double*, const int*, int, const int*, cudaStream_t);
 template int fermion_op<float>(const Geo&, int, const void*, const void*, const void*,
                                 const void*, void*, int, double, const void*, double,
-                                double*, const int*, int, cudaStream_t);
+                                double*, const int*, int, const int*, cudaStream_t);
 
 }  // namespace susy

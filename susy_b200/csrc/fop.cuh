@@ -21,6 +21,7 @@ struct FopArgs {
   const int* skip;  // device flag: nonzero = do nothing (finished solves)
   int comp_major;   // block order: 1 = all blocks of one output component together
   int nsb;          // site blocks per component
+  const int* nbrtab;  // neighbour index table of the table-driven variant
 };
 
 constexpr int FOP_THREADS = 128;

@@ -17,6 +17,10 @@ struct MsState {
   double zeta_i[MS_MAXS], zeta_im1[MS_MAXS], zeta_ip1[MS_MAXS];
   double beta_i[MS_MAXS], beta_im1[MS_MAXS], alpha[MS_MAXS];
   int converged[MS_MAXS], active_p[MS_MAXS];
+  // p_j update deferred to the next iteration's vector pass:
+  // p_j <- pz_j r + pa_j p_j when pact_j
+  double pz[MS_MAXS], pa[MS_MAXS];
+  int pact[MS_MAXS];
 };
 
 struct MsVecs {
@@ -30,15 +34,23 @@ struct MsVecs {
 // Kernel variants: matrix per thread with the 16 output components
 // interleaved block by block, the same with component-major block order,
 // and one matrix row per thread (component-major).
-enum { FOP_MAT = 0, FOP_MAT_CM = 1, FOP_ROWS = 2, FOP_NVARIANTS = 3 };
+// FOP_COMPACT evaluates all 220 products from a constant-memory term table;
+// FOP_COMPACT_PF also prefetches the next product's operands.
+enum { FOP_MAT = 0, FOP_MAT_CM = 1, FOP_ROWS = 2, FOP_COMPACT = 3, FOP_COMPACT_PF = 4,
+       FOP_NVARIANTS = 5 };
 template <typename R>
 int fermion_op(const Geo& g, int N, const void* U, const void* Uinv, const void* pd,
                 const void* src, void* dst, int sign, double G, const void* add, double addc,
-                double* dot, const int* skip, int variant, cudaStream_t st);
+                double* dot, const int* skip, int variant, const int* nbrtab, cudaStream_t st);
 template <typename R> struct FopArgs;
 template <typename R>
 int fermion_op_rows(const FopArgs<R>& a, int N, int sign, cudaStream_t st);
 int fop_partials(const Geo& g);
+template <typename R>
+int fermion_op_compact(const FopArgs<R>& a, int N, int sign, bool prefetch, cudaStream_t st);
+int upload_fop_terms(int device, cudaStream_t st);
+int fop_ndisp();
+void build_nbr_table(const Geo& g, int* tab, cudaStream_t st);
 
 // derived.cu
 void compute_uinv(const Geo& g, int N, const void* U, void* det, void* Uinv, cudaStream_t st);
@@ -66,6 +78,9 @@ int residual_partials(long n, const void* b, const void* ax, void* r64, void* r3
 void add_low(long n, const void* e32, void* x64, cudaStream_t s);
 void scale_field(long n, double sc, void* x, cudaStream_t s);
 void ms_update_b(MsState* st, const MsVecs& v, int prec, long n, cudaStream_t s);
+void ms_update_fused(MsState* st, const MsVecs& v, int prec, int prec_x, long n, double* part,
+                     cudaStream_t s);
+void ms_update_p0(MsState* st, const MsVecs& v, int prec, long n, cudaStream_t s);
 void norm2_partials(const void* x, int prec, long n, double* part, cudaStream_t s);
 
 }  // namespace susy

@@ -26,6 +26,7 @@ struct susy_b200_lattice {
   // FP32 copies read by the FP32 operator
   void *U32 = nullptr, *Uinv32 = nullptr, *pd32 = nullptr;
   void* stage = nullptr;  // AoS staging buffer (one FP64 Twist_Fermion)
+  int* nbrtab = nullptr;  // neighbour index table of the table-driven operator
   susy::MsState* ms = nullptr;
   void* tf64[SUSY_NSCRATCH] = {};
   void* tf32[SUSY_NSCRATCH] = {};

@@ -88,9 +88,9 @@ static int ms_run(susy_b200_lattice* h, const void* src, void* const* psim, int 
       dev_fop(h, p0, tmp, 1, pv, nullptr, 0.0, nullptr, skip);
       const int np_fop = dev_fop(h, tmp, mp, -1, pv, p0, fm2 + shift[0], part0, skip);
       ms_scalars1(h->ms, part0, np_fop, s);
-      ms_update_a(h->ms, v, pv, px, n, part1, s);
+      ms_update_fused(h->ms, v, pv, px, n, part1, s);
       ms_scalars2(h->ms, part1, np_vec, s);
-      ms_update_b(h->ms, v, pv, n, s);
+      ms_update_p0(h->ms, v, pv, n, s);
     }
     launched += chunk;
     cudaMemcpyAsync(pw, &h->ms->skip, sizeof(int), cudaMemcpyDeviceToHost, s);

@@ -385,7 +385,7 @@ class Lattice:
         """(current variant, autotuner ms per variant) for one precision."""
         ms = (C.c_float * 8)()
         v = self._check(self.lib.susy_b200_fop_variant(self.h, prec, set_to, ms))
-        return v, [ms[i] for i in range(3)]
+        return v, [ms[i] for i in range(5)]
 
     # ---- device-resident variants -----------------------------------------
     def tf(self, prec: int = 64) -> DeviceTF:

@@ -188,7 +188,7 @@ def test_operator_variants_agree(N):
     want = O.DSq(geo, prm, U, der, src)
     a, b = lat.tf(64), lat.tf(64)
     a.upload(synth.to_ref(dims, src))
-    for v in range(3):
+    for v in range(5):
         lat.fop_variant(64, v)
         lat.dev_DSq(a, b)
         assert rel(synth.from_ref(dims, b.download(), 16, N), want) < 1e-13, v
