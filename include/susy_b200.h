@@ -35,6 +35,8 @@ extern "C" {
 #define SUSY_B200_ENOMEM -3      /* device allocation failed             */
 #define SUSY_B200_ENOCONV -4     /* solver hit its iteration limit       */
 #define SUSY_B200_ENAN -5        /* non-finite value detected            */
+#define SUSY_B200_ESCRATCH -6    /* field larger than the fixed scratch of
+                                    susy_b200_DSq_noalloc                 */
 
 typedef struct susy_b200_lattice susy_b200_lattice;
 
@@ -128,6 +130,30 @@ int susy_b200_dev_fermion_op(susy_b200_lattice *h, const void *src, void *dst, i
 int susy_b200_autotune(susy_b200_lattice *h);
 int susy_b200_fop_variant(susy_b200_lattice *h, int prec, int set_to, float *ms_per_variant);
 int susy_b200_dev_DSq(susy_b200_lattice *h, const void *src, void *dst, int prec);
+/* dst = (D^dag D + fmass^2) src without allocating any device memory.
+ * No counterpart in the reference.  For callers that own every device
+ * buffer themselves and must not have a library call cudaMalloc (an
+ * application with its own device memory pool, or code that cannot afford
+ * the device-wide synchronisation an allocation may cause): no handle is
+ * needed and nothing is allocated, not even on the first call.  All
+ * pointers are FP64 device fields in the device layout (structure of
+ * arrays, lexicographic sites x + nx (y + ny (z + nz t)), site stride
+ * S = volume rounded up to a multiple of 32, complex {re, im} doubles):
+ *   links [5][ncol][ncol][S], src and dst [16][ncol][ncol][S];
+ *   Uinv [5][ncol][ncol][S] (inverse links) and plaqdet [25][S]
+ *   (plaquette determinants [a][b], as compute_plaqdet forms them) are read
+ *   only when G > 1e-8 and may be NULL otherwise.
+ * The intermediate field D src lives in one fixed 16 MiB device array inside
+ * the library (2^20 complex doubles, so 16 ncol^2 S <= 2^20, e.g. 8^4 sites
+ * for any ncol); larger lattices return SUSY_B200_ESCRATCH.  Every call on
+ * a device shares that array: calls whose kernels overlap on the GPU (other
+ * streams, other host threads) race and must be serialised by the caller.
+ * The first call on each device looks up the array's device address, so
+ * make that first call before any stream capture.  Launches on cuda_stream
+ * (NULL = default stream) and returns without synchronising. */
+int susy_b200_DSq_noalloc(int nx, int ny, int nz, int nt, int ncol, int pbc, double G,
+                          double fmass, const void *links, const void *Uinv,
+                          const void *plaqdet, const void *src, void *dst, void *cuda_stream);
 int susy_b200_dev_congrad_multi(susy_b200_lattice *h, const void *src, void *const *psim,
                                 int norder, const double *shift, int MaxCG, double errormin,
                                 double *size_r, int *iters);

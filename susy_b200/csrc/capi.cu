@@ -264,6 +264,7 @@ const char* susy_b200_error_string(int code) {
     case SUSY_B200_ENOMEM: return "device allocation failed";
     case SUSY_B200_ENOCONV: return "solver did not converge";
     case SUSY_B200_ENAN: return "non-finite value";
+    case SUSY_B200_ESCRATCH: return "field exceeds the 16 MiB scratch of susy_b200_DSq_noalloc";
     default: return "unknown error";
   }
 }
