@@ -343,6 +343,53 @@ def run_ours(args, rank, world, device):
     return line
 
 
+def run_dsq_case(args):
+    """Operator microbenchmark on the bench lattice: D^dag D per kernel
+    variant and precision (CUDA events on the launching stream, 20
+    applications after 3 warm-up ones; the 0.26 GB FP64 working set per
+    application is larger than L2).  --variant V restricts it to one variant
+    (the small case an ncu capture of one kernel runs)."""
+    import torch
+    from susy_b200 import Lattice, synth
+    from susy_b200.lattice import FOP_NVARIANTS
+    lat = Lattice(DIMS, NCOL, pbc=-1, lam=LAM, bmass=BMASS, G=G)
+    st = torch.cuda.Stream()
+    lat.set_stream(st.cuda_stream)
+    lat.set_links(synth.to_ref(DIMS, synth.links(DIMS, NCOL, LINK_NOISE, LINK_SEED)))
+    src = synth.to_ref(DIMS, synth.tf_source(DIMS, NCOL, SRC_SEED))
+    peak, peak_kind = measured_peaks()
+    variants = [args.variant] if args.variant >= 0 else list(range(FOP_NVARIANTS))
+    reps = 3 if args.variant >= 0 else 20
+    for prec, w in ((64, 16), (32, 8)):
+        a, b = lat.tf(prec), lat.tf(prec)
+        if prec == 64:
+            a.upload(src)
+        else:
+            a64 = lat.tf(64)
+            a64.upload(src)
+            lat.dev_convert(a64, a)
+        for v in variants:
+            lat.fop_variant(prec, v)
+            for _ in range(3):
+                lat.dev_DSq(a, b)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            for _ in range(reps):
+                lat.dev_DSq(a, b)
+            e1.record(st)
+            e1.synchronize()
+            ms = e0.elapsed_time(e1) / (2 * reps)
+            algo = algorithmic_bytes_fop(lat.V, NCOL, w)
+            gbs = algo / (ms * 1e-3) / 1e9
+            print(json.dumps({"case": "fermion_op", "lattice": "12x12x12x24", "ncol": NCOL,
+                              "prec": prec, "variant": v, "ms_per_launch": ms,
+                              "algorithmic_gbs": gbs, "frac": gbs / peak,
+                              "peak_kind": peak_kind,
+                              "tflops": flops_fop(lat.V, NCOL) / (ms * 1e-3) / 1e12}),
+                  flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -352,7 +399,13 @@ def main():
     ap.add_argument("--solver", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--dsq-case", action="store_true",
+                    help="operator microbenchmark per kernel variant instead of the solve")
+    ap.add_argument("--variant", type=int, default=-1)
     args = ap.parse_args()
+    if args.dsq_case:
+        run_dsq_case(args)
+        return
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

@@ -127,6 +127,14 @@ int susy_b200_dev_fermion_op(susy_b200_lattice *h, const void *src, void *dst, i
  * the fastest per precision; it also runs by itself on first use.
  * fop_variant returns the current variant of a precision, sets it when
  * set_to >= 0 and copies the autotuner's ms per variant when ms != NULL. */
+/* FP64 multi-shift CG vector update (no reference counterpart; the
+ * reference's congrad_multi.c:109-150 updates psi_j and p_j of every live
+ * shift every iteration).  on = 1 (default): one pass per 8 iterations
+ * advances every psi_j and p_j with the combined coefficients of those
+ * iterations (same recurrences and stopping rules, summed in a different
+ * order); on = 0: the per-iteration update.  on < 0 only queries.
+ * Returns the previous setting. */
+int susy_b200_cg_blocked(susy_b200_lattice *h, int on);
 int susy_b200_autotune(susy_b200_lattice *h);
 int susy_b200_fop_variant(susy_b200_lattice *h, int prec, int set_to, float *ms_per_variant);
 int susy_b200_dev_DSq(susy_b200_lattice *h, const void *src, void *dst, int prec);

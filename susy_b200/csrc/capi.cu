@@ -243,7 +243,7 @@ void susy_b200_destroy(susy_b200_lattice* h) {
   }
   for (int i = 0; i < SUSY_NPART; i++)
     if (h->part[i]) cudaFree(h->part[i]);
-  for (std::vector<void*>* v : {&h->extra, &h->sols, &h->pvec64, &h->pvec32, &h->gsrc,
+  for (std::vector<void*>* v : {&h->extra, &h->sols, &h->pvec64, &h->pvec32, &h->ring, &h->gsrc,
                                 &h->gr_psim, &h->traj_psim, &h->extra5, &h->refine})
     for (void* p : *v)
       if (p) cudaFree(p);
@@ -253,6 +253,13 @@ void susy_b200_destroy(susy_b200_lattice* h) {
 }
 
 long long susy_b200_launch_count(void) { return g_launches.load(); }
+
+int susy_b200_cg_blocked(susy_b200_lattice* h, int on) {
+  if (!h) return SUSY_B200_EINVAL;
+  const int prev = h->ms_blocked;
+  if (on >= 0) h->ms_blocked = on ? 1 : 0;
+  return prev;
+}
 
 int susy_b200_last_error(const susy_b200_lattice* h) { return h ? h->err : SUSY_B200_EINVAL; }
 

@@ -27,7 +27,7 @@ constexpr int UT = 256;
 constexpr int ST = 256;
 
 __global__ void k_ms_init(MsState* st, const double* partials, int np, int maxcg,
-                          double errormin) {
+                          double errormin, int record) {
   __shared__ double sh[ST];
   double v = 0.0;
   for (int i = threadIdx.x; i < np; i += ST) v += partials[i];
@@ -59,6 +59,10 @@ __global__ void k_ms_init(MsState* st, const double* partials, int np, int maxcg
     }
     st->skip = (st->rsq <= st->rsqstop || maxcg <= 0) ? 1 : 0;
     st->skip_b = 1;
+    st->record = record;
+    st->blk_len = 0;
+    st->blk_start = 0;
+    for (int j = 0; j < MS_MAXS; j++) st->live[j] = j < st->nshift;
   }
 }
 
@@ -114,6 +118,17 @@ __global__ void k_ms_scalars2(MsState* st, const double* partials, int np) {
     st->active_p[j] = !st->converged[j];
     if (st->converged[j]) continue;
     st->alpha[j] = a0 * st->zeta_ip1[j] * st->beta_i[j] / (st->zeta_i[j] * st->beta_i[0]);
+  }
+  if (st->record && st->blk_len < MS_BLK) {
+    // this iteration's coefficients, before this iteration's freeze test:
+    // a shift frozen in an earlier iteration took no step in this one
+    const int t = st->blk_len++;
+    for (int j = 0; j < st->nshift; j++) {
+      const bool live = j == 0 || !st->converged[j];
+      st->hb[t][j] = live ? st->beta_i[j] : 0.0;
+      st->hz[t][j] = j == 0 ? 1.0 : st->zeta_ip1[j];
+      st->ha[t][j] = st->alpha[j];
+    }
   }
   for (int j = 0; j < st->nshift; j++) {
     st->pz[j] = st->zeta_ip1[j];
@@ -284,13 +299,13 @@ __global__ void __launch_bounds__(UT) k_norm2(const VT* x, long n, double* part)
 int vec_blocks(long n) { return (int)((n + UT - 1) / UT); }
 
 void ms_init(MsState* st, const void* src, int prec, long n, double* part, int maxcg,
-             double errormin, cudaStream_t s) {
+             double errormin, cudaStream_t s, int record) {
   const int nb = vec_blocks(n);
   if (prec == 64)
     count_launch(), k_norm2<double2><<<nb, UT, 0, s>>>((const double2*)src, n, part);
   else
     count_launch(), k_norm2<float2><<<nb, UT, 0, s>>>((const float2*)src, n, part);
-  count_launch(), k_ms_init<<<1, ST, 0, s>>>(st, part, nb, maxcg, errormin);
+  count_launch(), k_ms_init<<<1, ST, 0, s>>>(st, part, nb, maxcg, errormin, record);
 }
 
 void ms_scalars1(MsState* st, const double* part, int np, cudaStream_t s) {
@@ -384,6 +399,156 @@ void ms_update_p0(MsState* st, const MsVecs& v, int prec, long n, cudaStream_t s
     count_launch(), k_ms_update_p0<double2><<<vec_blocks(n), UT, 0, s>>>(st, v, n);
   else
     count_launch(), k_ms_update_p0<float2><<<vec_blocks(n), UT, 0, s>>>(st, v, n);
+}
+
+// ---------------------------------------------------------------------------
+// Blocked update of the solutions and shifted search vectors.
+//
+// The per-iteration pass of the reference's recurrences reads and writes
+// psi_j and p_j of every live shift every iteration (4 field streams per
+// shift).  Over a block of L iterations starting at iteration k, with
+// R_s = r(k + s) the residuals the base recurrence produces,
+//   p_j(k + t) = c_t p_j(k) + sum_{s <= t} d_{t,s} R_s
+//   (c_0 = 1, c_{t+1} = a_t c_t, d_{t+1,s} = a_t d_{t,s}, d_{t+1,t+1} = z_t)
+//   psi_j(k + L) = psi_j(k) - sum_t b_t p_j(k + t)
+// with b_t, z_t, a_t shift j's beta, zeta(i+1), alpha of iteration k + t.
+// So one pass per block reads R_1..R_L once (shared by all shifts) and
+// psi_j, p_j once per shift: 4 streams per shift per L iterations instead
+// of per iteration.  The residual itself lives in a ring of L + 1 fields
+// so no copy is made.  Same arithmetic, summed in a different order.
+
+// r(i) = r(i-1) + beta_0 mp and partials of |r(i)|^2; i = iteration count
+// after this iteration's scalars1
+__global__ void __launch_bounds__(UT) k_msb_update_r(MsState* st, MsBlockVecs v, long n,
+                                                     double* part) {
+  if (st->skip) return;
+  const int it = st->iter;
+  const double b0 = st->beta_i[0];
+  const double2* rin = (const double2*)v.ring[(it - 1) % (MS_BLK + 1)];
+  double2* rout = (double2*)v.ring[it % (MS_BLK + 1)];
+  const long i = (long)blockIdx.x * UT + threadIdx.x;
+  double acc = 0.0;
+  if (i < n) {
+    double2 r = rin[i];
+    const double2 m = ((const double2*)v.mp)[i];
+    r.x += b0 * m.x;
+    r.y += b0 * m.y;
+    rout[i] = r;
+    acc = r.x * r.x + r.y * r.y;
+  }
+  acc = block_sum<UT>(acc);
+  if (threadIdx.x == 0) part[blockIdx.x] = acc;
+}
+
+// p0 = r(i) + alpha_0 p0
+__global__ void __launch_bounds__(UT) k_msb_update_p0(MsState* st, MsBlockVecs v, long n) {
+  if (st->skip_b) return;
+  const long i = (long)blockIdx.x * UT + threadIdx.x;
+  if (i >= n) return;
+  const double a0 = st->alpha[0];
+  const double2 r = ((const double2*)v.ring[st->iter % (MS_BLK + 1)])[i];
+  double2* pp = (double2*)v.p0 + i;
+  double2 p = *pp;
+  p.x = r.x + a0 * p.x;
+  p.y = r.y + a0 * p.y;
+  *pp = p;
+}
+
+// The block pass: every live shift's psi_j and P_j advanced over the
+// recorded iterations.  Each CTA first derives the combination
+// coefficients of every live shift in shared memory.
+__global__ void __launch_bounds__(UT) k_msb_block(MsState* st, MsBlockVecs v, long n) {
+  __shared__ double cx0[MS_MAXS], cp0[MS_MAXS];
+  __shared__ double cxr[MS_MAXS][MS_BLK], cpr[MS_MAXS][MS_BLK];
+  __shared__ int lv[MS_MAXS];
+  const int L = st->blk_len;
+  if (L == 0) return;
+  const int ns = st->nshift;
+  const int k = st->blk_start;
+  if (threadIdx.x < ns) {
+    const int j = threadIdx.x;
+    lv[j] = st->live[j];
+    // c_t and d_{t,s} for t = 0..L, s = 1..t (d indexed s-1)
+    double c = 1.0, d[MS_BLK];
+    double x0 = 0.0, xr[MS_BLK];
+#pragma unroll
+    for (int q = 0; q < MS_BLK; q++) d[q] = xr[q] = 0.0;
+    for (int t = 0; t < L; t++) {
+      const double b = st->hb[t][j], z = st->hz[t][j], a = st->ha[t][j];
+      // psi -= b_t p(k + t)
+      x0 += b * c;
+#pragma unroll
+      for (int q = 0; q < MS_BLK; q++)
+        if (q < t) xr[q] += b * d[q];
+      // p(k + t + 1) = z_t R_{t+1} + a_t p(k + t)
+      c *= a;
+#pragma unroll
+      for (int q = 0; q < MS_BLK; q++) {
+        if (q < t) d[q] *= a;
+        if (q == t) d[q] = z;
+      }
+    }
+    cx0[j] = x0;
+    cp0[j] = c;
+#pragma unroll
+    for (int q = 0; q < MS_BLK; q++) {
+      cxr[j][q] = xr[q];
+      cpr[j][q] = d[q];
+    }
+  }
+  __syncthreads();
+  const long i = (long)blockIdx.x * UT + threadIdx.x;
+  if (i >= n) return;
+  double2 R[MS_BLK];
+#pragma unroll
+  for (int q = 0; q < MS_BLK; q++)
+    R[q] = q < L ? ((const double2*)v.ring[(k + 1 + q) % (MS_BLK + 1)])[i] : make_double2(0, 0);
+#pragma unroll 1
+  for (int j = 0; j < ns; j++) {
+    if (!lv[j]) continue;
+    double2* pp = (double2*)v.P[j] + i;
+    double2* xp = (double2*)v.x[j] + i;
+    const double2 p = *pp;
+    double2 x = *xp;
+    double2 pn;
+    x.x -= cx0[j] * p.x;
+    x.y -= cx0[j] * p.y;
+    pn.x = cp0[j] * p.x;
+    pn.y = cp0[j] * p.y;
+#pragma unroll
+    for (int q = 0; q < MS_BLK; q++) {
+      x.x -= cxr[j][q] * R[q].x;
+      x.y -= cxr[j][q] * R[q].y;
+      pn.x += cpr[j][q] * R[q].x;
+      pn.y += cpr[j][q] * R[q].y;
+    }
+    *xp = x;
+    *pp = pn;
+  }
+}
+
+// Close the block: shifts frozen by now take no part in later blocks
+__global__ void k_msb_block_reset(MsState* st) {
+  const int j = threadIdx.x;
+  if (j < MS_MAXS) st->live[j] = j < st->nshift && (j == 0 || !st->converged[j]);
+  __syncthreads();
+  if (j == 0) {
+    st->blk_start = st->iter;
+    st->blk_len = 0;
+  }
+}
+
+void msb_update_r(MsState* st, const MsBlockVecs& v, long n, double* part, cudaStream_t s) {
+  count_launch(), k_msb_update_r<<<vec_blocks(n), UT, 0, s>>>(st, v, n, part);
+}
+
+void msb_update_p0(MsState* st, const MsBlockVecs& v, long n, cudaStream_t s) {
+  count_launch(), k_msb_update_p0<<<vec_blocks(n), UT, 0, s>>>(st, v, n);
+}
+
+void msb_block(MsState* st, const MsBlockVecs& v, long n, cudaStream_t s) {
+  count_launch(), k_msb_block<<<vec_blocks(n), UT, 0, s>>>(st, v, n);
+  count_launch(), k_msb_block_reset<<<1, MS_MAXS, 0, s>>>(st);
 }
 
 void norm2_partials(const void* x, int prec, long n, double* part, cudaStream_t s) {

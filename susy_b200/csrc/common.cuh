@@ -113,24 +113,93 @@ SUSY_D Cx<R> ldtr(const typename CT<R>::T* f, int k, int s, int S) {
 
 // ---------------------------------------------------------------------------
 // Matrix algebra in registers.  mode: 0 = A B, 1 = A B^dag, 2 = A^dag B
+// acc += s * op(A) op(B): the right factor is scaled once (2 N^2 multiplies)
+// and every complex multiply-add is four explicit fused multiply-adds into
+// the accumulator (written as sums of products, the compiler would round
+// each product and add separately).
 template <int M, int N, typename R>
 SUSY_D void mac(Mat<N, R>& acc, R s, const Mat<N, R>& A, const Mat<N, R>& B) {
+  Cx<R> bs[N][N];
+#pragma unroll
+  for (int k = 0; k < N; k++)
+#pragma unroll
+    for (int j = 0; j < N; j++) {
+      const Cx<R> b = (M == 1) ? conj(B.e[j][k]) : B.e[k][j];
+      bs[k][j] = Cx<R>(s * b.re, s * b.im);
+    }
 #pragma unroll
   for (int i = 0; i < N; i++)
 #pragma unroll
-    for (int j = 0; j < N; j++) {
-      R re = 0, im = 0;
+    for (int k = 0; k < N; k++) {
+      const Cx<R> a = (M == 2) ? conj(A.e[k][i]) : A.e[i][k];
 #pragma unroll
-      for (int k = 0; k < N; k++) {
-        Cx<R> a = (M == 2) ? conj(A.e[k][i]) : A.e[i][k];
-        Cx<R> b = (M == 1) ? conj(B.e[j][k]) : B.e[k][j];
-        re += a.re * b.re - a.im * b.im;
-        im += a.re * b.im + a.im * b.re;
+      for (int j = 0; j < N; j++) {
+        R re = acc.e[i][j].re, im = acc.e[i][j].im;
+        re = fma(a.re, bs[k][j].re, re);
+        re = fma(-a.im, bs[k][j].im, re);
+        im = fma(a.re, bs[k][j].im, im);
+        im = fma(a.im, bs[k][j].re, im);
+        acc.e[i][j] = Cx<R>(re, im);
       }
-      acc.e[i][j].re += s * re;
-      acc.e[i][j].im += s * im;
     }
 }
+
+// FP32 accumulator for the operator kernels in packed-pair arithmetic
+// (two FP32 lanes per instruction, sm_100): P = sum a.re * b and
+// Q = sum a.im * b as (re, im) pairs, so a product a b = (P.x - Q.y,
+// P.y + Q.x) costs two pair-FMAs per complex multiply-add.
+template <int N>
+struct AccPair {
+  float2 P[N][N], Q[N][N];
+  SUSY_D void zero() {
+#pragma unroll
+    for (int i = 0; i < N; i++)
+#pragma unroll
+      for (int j = 0; j < N; j++) P[i][j] = Q[i][j] = make_float2(0.f, 0.f);
+  }
+  // += s * A B
+  SUSY_D void add(float s, const Mat<N, float>& A, const Mat<N, float>& B) {
+    float2 bs[N][N];
+    const float2 ss = make_float2(s, s);
+#pragma unroll
+    for (int k = 0; k < N; k++)
+#pragma unroll
+      for (int j = 0; j < N; j++) bs[k][j] = __fmul2_rn(make_float2(B.e[k][j].re, B.e[k][j].im), ss);
+#pragma unroll
+    for (int i = 0; i < N; i++)
+#pragma unroll
+      for (int k = 0; k < N; k++) {
+        const float2 ar = make_float2(A.e[i][k].re, A.e[i][k].re);
+        const float2 ai = make_float2(A.e[i][k].im, A.e[i][k].im);
+#pragma unroll
+        for (int j = 0; j < N; j++) {
+          P[i][j] = __ffma2_rn(ar, bs[k][j], P[i][j]);
+          Q[i][j] = __ffma2_rn(ai, bs[k][j], Q[i][j]);
+        }
+      }
+  }
+  SUSY_D Mat<N, float> get() const {
+    Mat<N, float> m;
+#pragma unroll
+    for (int i = 0; i < N; i++)
+#pragma unroll
+      for (int j = 0; j < N; j++)
+        m.e[i][j] = Cx<float>(P[i][j].x - Q[i][j].y, P[i][j].y + Q[i][j].x);
+    return m;
+  }
+};
+
+// Plain accumulator with the same interface (FP64)
+template <int N, typename R>
+struct AccMat {
+  Mat<N, R> m;
+  SUSY_D void zero() { m.zero(); }
+  SUSY_D void add(R s, const Mat<N, R>& A, const Mat<N, R>& B) { mac<0>(m, s, A, B); }
+  SUSY_D Mat<N, R> get() const { return m; }
+};
+
+template <int N, typename R> struct AccOf { typedef AccMat<N, R> T; };
+template <int N> struct AccOf<N, float> { typedef AccPair<N> T; };
 
 template <int N, typename R>
 SUSY_D void axpy(Mat<N, R>& acc, Cx<R> c, const Mat<N, R>& A) {

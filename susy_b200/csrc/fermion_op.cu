@@ -276,8 +276,7 @@ int fermion_op(const Geo& g, int N, const void* U, const void* Uinv, const void*
   a.skip = skip;
   a.nbrtab = nbrtab;
   if (variant == FOP_ROWS) return fermion_op_rows<R>(a, N, sign, st);
-  if (variant == FOP_COMPACT || variant == FOP_COMPACT_PF)
-    return fermion_op_compact<R>(a, N, sign, variant == FOP_COMPACT_PF, st);
+  if (variant >= FOP_COMPACT) return fermion_op_compact<R>(a, N, sign, variant, st);
   a.comp_major = variant == FOP_MAT_CM;
   switch (N) {
     case 2: return launch_fop<2, R, 1>(a, sign, st);

@@ -321,6 +321,124 @@ fermion_op_compact_kernel(FopArgs<R> a) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// Second generation of the table-driven kernels.
+//
+// Site-major block order: the 16 blocks of one site tile (one per output
+// component) are adjacent in the grid, so they run at the same time and
+// the tile's neighbourhood (source, links, U^-1, plaquette determinants
+// within three steps) is fetched from HBM once and then served from L2 to
+// all 16; with component-major order every output component sweeps the
+// whole lattice and the links are re-read from HBM per component.
+//
+// Two operand buffers used alternately: the next product's operands are in
+// flight while the current one is multiplied, with no register copies
+// between iterations (a rolled loop with one prefetch buffer copies both
+// matrices every term).  Both block orders are built; which one wins
+// depends on the precision (the autotuner decides).  In FP32 the products
+// run in packed-pair arithmetic (AccPair, common.cuh).
+
+// Shared epilogue: determinant terms, adjoint for D^dag, axpy and dot
+template <int N, typename R, int SIGN>
+SUSY_D double fop_finish(Mat<N, R>& acc, const FopArgs<R>& a, const Site& c, int comp) {
+  if (a.doG) {
+    if (comp == 0)
+      det_ltos_rt<N, R, SIGN>(acc, a, c);
+    else if (comp <= NUMLINK)
+      det_stol_rt<N, R, SIGN>(acc, a, c, comp - 1);
+  }
+  if (SIGN < 0) {
+    Mat<N, R> t = acc;
+#pragma unroll
+    for (int i = 0; i < N; i++)
+#pragma unroll
+      for (int j = 0; j < N; j++) acc.e[i][j] = Cx<R>(-t.e[j][i].re, t.e[j][i].im);
+  }
+  double part = 0.0;
+  if (a.add) {
+    Mat<N, R> x = ldm<N, R>(a.add, comp, c.s, a.g.S);
+    axpy(acc, Cx<R>(a.addc, 0), x);
+    if (a.dot) part = rdot(x, acc);
+  }
+  stm<N, R>(a.dst, comp, c.s, a.g.S, acc);
+  return part;
+}
+
+// PP = false: one operand buffer, no prefetch (fewest registers)
+template <int N, typename R, int SIGN, int PAT, bool PP, typename ACC>
+SUSY_D void run_pattern_pp(ACC& acc, const FopArgs<R>& a, int s, unsigned bcm, int t0, int t1) {
+  constexpr bool LF = (PAT == P_FU || PAT == P_FUD);
+  constexpr bool RF = !LF;
+  constexpr bool AL = (PAT == P_UDF) ^ (LF && SIGN < 0);
+  constexpr bool AR = (PAT == P_FUD) ^ (RF && SIGN < 0);
+  const int S = a.g.S;
+  const typename CT<R>::T* fl = LF ? a.src : a.U;
+  const typename CT<R>::T* fr = RF ? a.src : a.U;
+  const R pbc = (R)a.g.pbc;
+  if (t0 >= t1) return;
+  if (!PP) {
+#pragma unroll 1
+    for (int t = t0; t < t1; t++) {
+      const FTerm T = c_terms[t];
+      const Mat<N, R> L = ldm<N, R, AL>(fl, T.kl, a.nbrtab[(size_t)T.dl * S + s], S);
+      const Mat<N, R> Rm = ldm<N, R, AR>(fr, T.kr, a.nbrtab[(size_t)T.dr * S + s], S);
+      acc.add((R)T.coef * bc_of<R>(bcm, T.bcdt, pbc), L, Rm);
+    }
+    return;
+  }
+  FTerm TA = c_terms[t0];
+  Mat<N, R> LA = ldm<N, R, AL>(fl, TA.kl, a.nbrtab[(size_t)TA.dl * S + s], S);
+  Mat<N, R> RA = ldm<N, R, AR>(fr, TA.kr, a.nbrtab[(size_t)TA.dr * S + s], S);
+#pragma unroll 1
+  for (int t = t0;; t += 2) {
+    FTerm TB;
+    Mat<N, R> LB, RB;
+    const bool hb = t + 1 < t1;
+    if (hb) {
+      TB = c_terms[t + 1];
+      LB = ldm<N, R, AL>(fl, TB.kl, a.nbrtab[(size_t)TB.dl * S + s], S);
+      RB = ldm<N, R, AR>(fr, TB.kr, a.nbrtab[(size_t)TB.dr * S + s], S);
+    }
+    acc.add((R)TA.coef * bc_of<R>(bcm, TA.bcdt, pbc), LA, RA);
+    if (!hb) break;
+    const bool ha = t + 2 < t1;
+    if (ha) {
+      TA = c_terms[t + 2];
+      LA = ldm<N, R, AL>(fl, TA.kl, a.nbrtab[(size_t)TA.dl * S + s], S);
+      RA = ldm<N, R, AR>(fr, TA.kr, a.nbrtab[(size_t)TA.dr * S + s], S);
+    }
+    acc.add((R)TB.coef * bc_of<R>(bcm, TB.bcdt, pbc), LB, RB);
+    if (!ha) break;
+  }
+}
+
+// Block order: site-major (SM = true) or component-major.  FP32 accumulates
+// in packed pairs (AccPair), FP64 in a plain matrix.
+template <int N, typename R, int SIGN, bool SM, bool PP>
+__global__ void __launch_bounds__(CT_THREADS)
+fermion_op_pp_kernel(FopArgs<R> a) {
+  if (a.skip && *a.skip) return;
+  const int comp = SM ? blockIdx.x % NTF : blockIdx.x / a.nsb;
+  const int s = (SM ? blockIdx.x / NTF : blockIdx.x % a.nsb) * CT_THREADS + threadIdx.x;
+  double part = 0.0;
+  if (s < a.g.V) {
+    const Site c = site_of(a.g, s);
+    const unsigned bcm = bc_mask(a.g, c);
+    typename AccOf<N, R>::T acc;
+    acc.zero();
+    run_pattern_pp<N, R, SIGN, P_UF, PP>(acc, a, s, bcm, c_pat_start[comp][0], c_pat_start[comp][1]);
+    run_pattern_pp<N, R, SIGN, P_FU, PP>(acc, a, s, bcm, c_pat_start[comp][1], c_pat_start[comp][2]);
+    run_pattern_pp<N, R, SIGN, P_FUD, PP>(acc, a, s, bcm, c_pat_start[comp][2], c_pat_start[comp][3]);
+    run_pattern_pp<N, R, SIGN, P_UDF, PP>(acc, a, s, bcm, c_pat_start[comp][3], c_pat_start[comp][4]);
+    Mat<N, R> out = acc.get();
+    part = fop_finish<N, R, SIGN>(out, a, c, comp);
+  }
+  if (a.dot) {
+    part = block_sum<CT_THREADS>(part);
+    if (threadIdx.x == 0) a.dot[blockIdx.x] = part;
+  }
+}
+
 template <int N, typename R, bool PF>
 static int launch_compact(FopArgs<R> a, int sign, cudaStream_t st) {
   a.nsb = (a.g.V + CT_THREADS - 1) / CT_THREADS;
@@ -332,19 +450,51 @@ static int launch_compact(FopArgs<R> a, int sign, cudaStream_t st) {
   return nblk;
 }
 
+template <int N, typename R, bool SM, bool PP>
+static int launch_pp(FopArgs<R> a, int sign, cudaStream_t st) {
+  a.nsb = (a.g.V + CT_THREADS - 1) / CT_THREADS;
+  const int nblk = a.nsb * NTF;
+  if (sign > 0)
+    count_launch(), fermion_op_pp_kernel<N, R, 1, SM, PP><<<nblk, CT_THREADS, 0, st>>>(a);
+  else
+    count_launch(), fermion_op_pp_kernel<N, R, -1, SM, PP><<<nblk, CT_THREADS, 0, st>>>(a);
+  return nblk;
+}
+
 template <typename R>
-int fermion_op_compact(const FopArgs<R>& a, int N, int sign, bool prefetch, cudaStream_t st) {
-  switch (N) {
-    case 2: return prefetch ? launch_compact<2, R, true>(a, sign, st)
-                            : launch_compact<2, R, false>(a, sign, st);
-    case 3: return prefetch ? launch_compact<3, R, true>(a, sign, st)
-                            : launch_compact<3, R, false>(a, sign, st);
-    default: return prefetch ? launch_compact<4, R, true>(a, sign, st)
-                             : launch_compact<4, R, false>(a, sign, st);
+int fermion_op_compact(const FopArgs<R>& a, int N, int sign, int variant, cudaStream_t st) {
+  switch (variant) {
+    case FOP_COMPACT:
+    case FOP_COMPACT_PF: {
+      const bool pf = variant == FOP_COMPACT_PF;
+      switch (N) {
+        case 2: return pf ? launch_compact<2, R, true>(a, sign, st) : launch_compact<2, R, false>(a, sign, st);
+        case 3: return pf ? launch_compact<3, R, true>(a, sign, st) : launch_compact<3, R, false>(a, sign, st);
+        default: return pf ? launch_compact<4, R, true>(a, sign, st) : launch_compact<4, R, false>(a, sign, st);
+      }
+    }
+    case FOP_SITE_MAJOR_PP:
+      switch (N) {
+        case 2: return launch_pp<2, R, true, true>(a, sign, st);
+        case 3: return launch_pp<3, R, true, true>(a, sign, st);
+        default: return launch_pp<4, R, true, true>(a, sign, st);
+      }
+    case FOP_COMP_MAJOR_PP:
+      switch (N) {
+        case 2: return launch_pp<2, R, false, true>(a, sign, st);
+        case 3: return launch_pp<3, R, false, true>(a, sign, st);
+        default: return launch_pp<4, R, false, true>(a, sign, st);
+      }
+    default:
+      switch (N) {
+        case 2: return launch_pp<2, R, false, false>(a, sign, st);
+        case 3: return launch_pp<3, R, false, false>(a, sign, st);
+        default: return launch_pp<4, R, false, false>(a, sign, st);
+      }
   }
 }
 
-template int fermion_op_compact<double>(const FopArgs<double>&, int, int, bool, cudaStream_t);
-template int fermion_op_compact<float>(const FopArgs<float>&, int, int, bool, cudaStream_t);
+template int fermion_op_compact<double>(const FopArgs<double>&, int, int, int, cudaStream_t);
+template int fermion_op_compact<float>(const FopArgs<float>&, int, int, int, cudaStream_t);
 
 }  // namespace susy

@@ -8,11 +8,20 @@
 namespace susy {
 
 constexpr int MS_MAXS = 32;
+// Iterations per block of the blocked solution/search-vector update
+constexpr int MS_BLK = 8;
 
 // Device-resident state of one multi-shift solve (FP64 scalars)
 struct MsState {
   double rsq, rsqstop, source_norm, cd;
   int iter, maxcg, nshift, skip, skip_b, pad;
+  // blocked update: per-iteration coefficients of the current block
+  // (hb = beta_j, 0 once shift j is frozen; hz = zeta_j(i+1); ha = alpha_j),
+  // iterations recorded so far, iteration count at the block start, and
+  // the shifts still live when the block began
+  int record, blk_len, blk_start, pad2;
+  int live[MS_MAXS];
+  double hb[MS_BLK][MS_MAXS], hz[MS_BLK][MS_MAXS], ha[MS_BLK][MS_MAXS];
   double shift[MS_MAXS];
   double zeta_i[MS_MAXS], zeta_im1[MS_MAXS], zeta_ip1[MS_MAXS];
   double beta_i[MS_MAXS], beta_im1[MS_MAXS], alpha[MS_MAXS];
@@ -30,14 +39,30 @@ struct MsVecs {
   void* mp;
 };
 
+// Vectors of the blocked solver: ring[i % (MS_BLK + 1)] holds the residual
+// after i iterations; P[j] is shift j's search vector at the block start
+// (P[0] a copy of the operator input p0 at that point); x[j] the solutions.
+struct MsBlockVecs {
+  void* ring[MS_BLK + 1];
+  void* P[MS_MAXS];
+  void* x[MS_MAXS];
+  void* p0;
+  void* mp;
+};
+
 // fermion_op.cu, fermion_op_rows.cu
 // Kernel variants: matrix per thread with the 16 output components
 // interleaved block by block, the same with component-major block order,
 // and one matrix row per thread (component-major).
 // FOP_COMPACT evaluates all 220 products from a constant-memory term table;
 // FOP_COMPACT_PF also prefetches the next product's operands.
+// FOP_SITE_MAJOR_PP / FOP_COMP_MAJOR_PP: table-driven with two alternating
+// operand buffers, site-major or component-major block order, FP32 in
+// packed-pair arithmetic; FOP_COMP_MAJOR_PAIR: the same component-major
+// kernel with one operand buffer (fewest registers).
 enum { FOP_MAT = 0, FOP_MAT_CM = 1, FOP_ROWS = 2, FOP_COMPACT = 3, FOP_COMPACT_PF = 4,
-       FOP_NVARIANTS = 5 };
+       FOP_SITE_MAJOR_PP = 5, FOP_COMP_MAJOR_PP = 6, FOP_COMP_MAJOR_PAIR = 7,
+       FOP_NVARIANTS = 8 };
 template <typename R>
 int fermion_op(const Geo& g, int N, const void* U, const void* Uinv, const void* pd,
                 const void* src, void* dst, int sign, double G, const void* add, double addc,
@@ -47,7 +72,7 @@ template <typename R>
 int fermion_op_rows(const FopArgs<R>& a, int N, int sign, cudaStream_t st);
 int fop_partials(const Geo& g);
 template <typename R>
-int fermion_op_compact(const FopArgs<R>& a, int N, int sign, bool prefetch, cudaStream_t st);
+int fermion_op_compact(const FopArgs<R>& a, int N, int sign, int variant, cudaStream_t st);
 int upload_fop_terms(int device, cudaStream_t st);
 int fop_ndisp();
 void build_nbr_table(const Geo& g, int* tab, cudaStream_t st);
@@ -68,7 +93,7 @@ void convert_field(long ncomplex, const void* in, int prec_in, void* out, int pr
 // cg.cu
 int vec_blocks(long n);
 void ms_init(MsState* st, const void* src, int prec, long n, double* part, int maxcg,
-             double errormin, cudaStream_t s);
+             double errormin, cudaStream_t s, int record = 0);
 void ms_scalars1(MsState* st, const double* part, int np, cudaStream_t s);
 void ms_scalars2(MsState* st, const double* part, int np, cudaStream_t s);
 void ms_update_a(MsState* st, const MsVecs& v, int prec, int prec_x, long n, double* part,
@@ -82,6 +107,9 @@ void ms_update_fused(MsState* st, const MsVecs& v, int prec, int prec_x, long n,
                      cudaStream_t s);
 void ms_update_p0(MsState* st, const MsVecs& v, int prec, long n, cudaStream_t s);
 void norm2_partials(const void* x, int prec, long n, double* part, cudaStream_t s);
+void msb_update_r(MsState* st, const MsBlockVecs& v, long n, double* part, cudaStream_t s);
+void msb_update_p0(MsState* st, const MsBlockVecs& v, long n, cudaStream_t s);
+void msb_block(MsState* st, const MsBlockVecs& v, long n, cudaStream_t s);
 
 }  // namespace susy
 

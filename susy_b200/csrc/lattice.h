@@ -34,6 +34,8 @@ struct susy_b200_lattice {
   std::vector<void*> sols;    // solutions for the host-facing CG
   std::vector<void*> pvec64;  // p_j of the FP64 multi-shift CG
   std::vector<void*> pvec32;
+  std::vector<void*> ring;    // residual ring of the blocked FP64 solver
+  int ms_blocked = 1;         // FP64 multi-shift CG: blocked vector update
   std::vector<void*> extra;   // other lazily allocated fields
   int* poll = nullptr;        // pinned host words for solver polling
   // trajectory state (hmc.cu)

@@ -108,10 +108,88 @@ static int ms_run(susy_b200_lattice* h, const void* src, void* const* psim, int 
   return SUSY_B200_OK;
 }
 
+static void* ring_field(susy_b200_lattice* h, int q) {
+  while ((int)h->ring.size() <= q) h->ring.push_back(dalloc(h, field_bytes(h, NTF, 64)));
+  return h->ring[q];
+}
+
+// FP64 multi-shift CG with the blocked solution / search-vector update
+// (cg.cu k_msb_block): the reference's recurrences and stopping rules,
+// the shifted vectors touched once per MS_BLK iterations.
+static int ms_run_block(susy_b200_lattice* h, const void* src, void* const* psim, int norder,
+                        const double* shift, int MaxCG, double errormin, double* size_r,
+                        int* iters) {
+  cudaStream_t s = h->stream;
+  const long n = tf_complex(h);
+  const size_t bv = field_bytes(h, NTF, 64);
+  void* p0 = scratch_tf(h, 3, 64);
+  void* mp = scratch_tf(h, 5, 64);
+  void* tmp = scratch_tf(h, 0, 64);
+  double* part0 = partials(h, 0);
+  double* part1 = partials(h, 1);
+  int* pw = poll_words(h);
+  if (!p0 || !mp || !tmp || !part0 || !part1 || !pw) return set_err(h, SUSY_B200_ENOMEM);
+  MsBlockVecs v;
+  for (int q = 0; q <= MS_BLK; q++) {
+    v.ring[q] = ring_field(h, q);
+    if (!v.ring[q]) return set_err(h, SUSY_B200_ENOMEM);
+  }
+  for (int j = 0; j < norder; j++) {
+    v.P[j] = pvec(h, j, 64);
+    if (!v.P[j]) return set_err(h, SUSY_B200_ENOMEM);
+    v.x[j] = psim[j];
+  }
+  v.p0 = p0;
+  v.mp = mp;
+  // r(0) = src, p0 = P_j = src, psi_j = 0   (congrad_multi.c:47-57)
+  cudaMemcpyAsync(v.ring[0], src, bv, cudaMemcpyDeviceToDevice, s);
+  cudaMemcpyAsync(p0, src, bv, cudaMemcpyDeviceToDevice, s);
+  for (int j = 0; j < norder; j++) {
+    cudaMemcpyAsync(v.P[j], src, bv, cudaMemcpyDeviceToDevice, s);
+    cudaMemsetAsync(psim[j], 0, bv, s);
+  }
+  int ns = norder;
+  cudaMemcpyAsync(&h->ms->nshift, &ns, sizeof(int), cudaMemcpyHostToDevice, s);
+  cudaMemcpyAsync(h->ms->shift, shift, sizeof(double) * norder, cudaMemcpyHostToDevice, s);
+  ms_init(h->ms, src, 64, n, part0, MaxCG, errormin, s, 1);
+
+  const double fm2 = h->prm.fmass > 1e-8 ? h->prm.fmass * h->prm.fmass : 0.0;
+  const int np_vec = vec_blocks(n);
+  const int* skip = &h->ms->skip;
+  const int chunk = 2 * MS_BLK;
+  int launched = 0;
+  for (;;) {
+    for (int k = 0; k < chunk; k++) {
+      dev_fop(h, p0, tmp, 1, 64, nullptr, 0.0, nullptr, skip);
+      const int np_fop = dev_fop(h, tmp, mp, -1, 64, p0, fm2 + shift[0], part0, skip);
+      ms_scalars1(h->ms, part0, np_fop, s);
+      msb_update_r(h->ms, v, n, part1, s);
+      ms_scalars2(h->ms, part1, np_vec, s);
+      msb_update_p0(h->ms, v, n, s);
+      if ((k + 1) % MS_BLK == 0) msb_block(h->ms, v, n, s);
+    }
+    launched += chunk;
+    cudaMemcpyAsync(pw, &h->ms->skip, sizeof(int), cudaMemcpyDeviceToHost, s);
+    if (!ck(h, cudaStreamSynchronize(s))) return SUSY_B200_ECUDA;
+    if (pw[0] || launched >= MaxCG + chunk) break;
+  }
+  double rsq = 0.0;
+  int it = 0;
+  cudaMemcpyAsync(&rsq, &h->ms->rsq, sizeof(double), cudaMemcpyDeviceToHost, s);
+  cudaMemcpyAsync(&it, &h->ms->iter, sizeof(int), cudaMemcpyDeviceToHost, s);
+  if (!ck(h, cudaStreamSynchronize(s))) return SUSY_B200_ECUDA;
+  if (!(rsq == rsq)) return set_err(h, SUSY_B200_ENAN);
+  if (size_r) *size_r = rsq;
+  if (iters) *iters = it;
+  return SUSY_B200_OK;
+}
+
 // Reference-faithful FP64 multi-shift CG (congrad_multi.c:26-221)
 int multishift_fp64(susy_b200_lattice* h, const void* src, void* const* psim, int norder,
                     const double* shift, int MaxCG, double errormin, double* size_r,
                     int* iters) {
+  if (h->ms_blocked)
+    return ms_run_block(h, src, psim, norder, shift, MaxCG, errormin, size_r, iters);
   return ms_run(h, src, psim, norder, shift, MaxCG, errormin, 64, 64, size_r, iters);
 }
 

@@ -46,6 +46,7 @@ class TrajResult(C.Structure):
 
 SOLVER_FP64 = 0
 SOLVER_MIXED = 1
+FOP_NVARIANTS = 8
 
 
 class RHMC:
@@ -125,6 +126,8 @@ def load_library(path: str = LIB_PATH):
     L.susy_b200_dev_DSq.argtypes = [_vp, _vp, _vp, C.c_int]
     L.susy_b200_autotune.argtypes = [_vp]
     L.susy_b200_fop_variant.argtypes = [_vp, C.c_int, C.c_int, C.POINTER(C.c_float)]
+    L.susy_b200_cg_blocked.restype = C.c_int
+    L.susy_b200_cg_blocked.argtypes = [_vp, C.c_int]
     L.susy_b200_dev_congrad_multi.argtypes = [_vp, _vp, C.POINTER(_vp), C.c_int, _dp, C.c_int,
                                               C.c_double, _dp, C.POINTER(C.c_int)]
     L.susy_b200_dev_congrad_multi_mixed.argtypes = [_vp, _vp, C.POINTER(_vp), C.c_int, _dp,
@@ -381,11 +384,16 @@ class Lattice:
     def autotune(self):
         self._check(self.lib.susy_b200_autotune(self.h))
 
+    def cg_blocked(self, on: int = -1) -> int:
+        """Blocked (1) or per-iteration (0) vector update of the FP64
+        multi-shift CG; returns the previous setting (on < 0 only queries)."""
+        return self._check(self.lib.susy_b200_cg_blocked(self.h, int(on)))
+
     def fop_variant(self, prec: int = 64, set_to: int = -1):
         """(current variant, autotuner ms per variant) for one precision."""
         ms = (C.c_float * 8)()
         v = self._check(self.lib.susy_b200_fop_variant(self.h, prec, set_to, ms))
-        return v, [ms[i] for i in range(5)]
+        return v, [ms[i] for i in range(FOP_NVARIANTS)]
 
     # ---- device-resident variants -----------------------------------------
     def tf(self, prec: int = 64) -> DeviceTF:

@@ -51,3 +51,28 @@ def test_congrad_multi_maxcg_returns_iterations():
     psim = [np.zeros(lat.tf_doubles) for _ in shifts]
     it, rsq = lat.congrad_multi(src, psim, shifts, 7, 1e-20)
     assert it == 7 and rsq > 0
+
+
+@pytest.mark.parametrize("maxcg,errormin", [(5000, 1e-20), (13, 1e-20), (7, 1e-20),
+                                            (5000, 1e-8)])
+def test_blocked_update_matches_per_iteration(maxcg, errormin):
+    """The blocked vector update (one pass per 8 iterations) against the
+    per-iteration update of congrad_multi.c:109-150: same iteration count,
+    same iterated residual and solutions to 1e-11 relative, including solves
+    that end inside a block (MaxCG 7 and 13) and shifts that freeze
+    mid-block (the loose 1e-8 stop)."""
+    dims, N = (4, 4, 4, 4), 3
+    lat = Lattice(dims, N, pbc=-1, G=0.05)
+    lat.set_links(synth.to_ref(dims, synth.links(dims, N, 0.2, 4)))
+    src = synth.to_ref(dims, synth.tf_source(dims, N, seed=8))
+    shifts = synth.geometric_shifts(15, 1e-5, 1e3)
+    out = {}
+    for on in (0, 1):
+        lat.cg_blocked(on)
+        psim = [np.zeros(lat.tf_doubles) for _ in shifts]
+        it, rsq = lat.congrad_multi(src, psim, shifts, maxcg, errormin)
+        out[on] = (it, rsq, psim)
+    assert out[0][0] == out[1][0]
+    assert abs(out[0][1] - out[1][1]) <= 1e-9 * out[0][1]
+    for a, b in zip(out[0][2], out[1][2]):
+        assert np.abs(a - b).max() <= 1e-11 * np.abs(a).max()

@@ -179,8 +179,13 @@ def test_mixed_solver_reaches_fp64_residual(N):
         assert O.magsq(res) <= 1.5 * errormin * b2
 
 
-@pytest.mark.parametrize("N", [2, 3])
+@pytest.mark.parametrize("N", [2, 3, 4])
 def test_operator_variants_agree(N):
+    """Every operator kernel variant against the oracle: D^dag D in FP64 to
+    1e-13 and in FP32 to 2e-6 (relative, max-norm), and one short FP64
+    multi-shift solve through each variant (the operator's fused
+    axpy + dot epilogue) to the same iteration count and stopping bound."""
+    from susy_b200.lattice import FOP_NVARIANTS
     dims = (4, 4, 4, 8)
     lat, geo, prm, U = make(dims, N, G=0.05)
     der = O.compute_derived(geo, prm, U)
@@ -188,7 +193,23 @@ def test_operator_variants_agree(N):
     want = O.DSq(geo, prm, U, der, src)
     a, b = lat.tf(64), lat.tf(64)
     a.upload(synth.to_ref(dims, src))
-    for v in range(5):
+    a32, b32 = lat.tf(32), lat.tf(32)
+    lat.dev_convert(a, a32)
+    shifts = np.array([1e-3, 0.1, 2.0])
+    psim = [lat.tf(64) for _ in shifts]
+    solves = []
+    for v in range(FOP_NVARIANTS):
         lat.fop_variant(64, v)
+        lat.fop_variant(32, v)
         lat.dev_DSq(a, b)
         assert rel(synth.from_ref(dims, b.download(), 16, N), want) < 1e-13, v
+        lat.dev_DSq(a32, b32)
+        lat.dev_convert(b32, b)
+        assert rel(synth.from_ref(dims, b.download(), 16, N), want) < 2e-6, v
+        it, rsq = lat.dev_congrad_multi(a, psim, shifts, 500, 1e-16)
+        solves.append((it, rsq))
+    # variants sum the products in different orders: rounding may move the
+    # stopping iteration by one
+    assert all(abs(x[0] - solves[0][0]) <= 1 for x in solves), solves
+    b2 = O.magsq(src)
+    assert all(x[1] <= 1e-16 * b2 for x in solves), solves
