@@ -135,6 +135,12 @@ int susy_b200_dev_fermion_op(susy_b200_lattice *h, const void *src, void *dst, i
  * order); on = 0: the per-iteration update.  on < 0 only queries.
  * Returns the previous setting. */
 int susy_b200_cg_blocked(susy_b200_lattice *h, int on);
+/* Mixed-precision solver settings (no reference counterpart): the operator
+ * runs in FP32 once |r| < fp32_below |src| (default 3e-4); with the FP32
+ * operator the FP64 true residual replaces the iterated one whenever |r|
+ * fell by reliable_factor (default 1e-2) since the last replacement.
+ * 0 < fp32_below <= 1, 0 < reliable_factor < 1, else SUSY_B200_EINVAL. */
+int susy_b200_mixed_params(susy_b200_lattice *h, double fp32_below, double reliable_factor);
 int susy_b200_autotune(susy_b200_lattice *h);
 int susy_b200_fop_variant(susy_b200_lattice *h, int prec, int set_to, float *ms_per_variant);
 int susy_b200_dev_DSq(susy_b200_lattice *h, const void *src, void *dst, int prec);

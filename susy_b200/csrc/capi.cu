@@ -254,6 +254,15 @@ void susy_b200_destroy(susy_b200_lattice* h) {
 
 long long susy_b200_launch_count(void) { return g_launches.load(); }
 
+int susy_b200_mixed_params(susy_b200_lattice* h, double fp32_below, double reliable_factor) {
+  if (!h || !(fp32_below > 0.0 && fp32_below <= 1.0) ||
+      !(reliable_factor > 0.0 && reliable_factor < 1.0))
+    return SUSY_B200_EINVAL;
+  h->mix_switch = fp32_below;
+  h->mix_reliable = reliable_factor;
+  return SUSY_B200_OK;
+}
+
 int susy_b200_cg_blocked(susy_b200_lattice* h, int on) {
   if (!h) return SUSY_B200_EINVAL;
   const int prev = h->ms_blocked;

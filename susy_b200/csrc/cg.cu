@@ -418,7 +418,9 @@ void ms_update_p0(MsState* st, const MsVecs& v, int prec, long n, cudaStream_t s
 // so no copy is made.  Same arithmetic, summed in a different order.
 
 // r(i) = r(i-1) + beta_0 mp and partials of |r(i)|^2; i = iteration count
-// after this iteration's scalars1
+// after this iteration's scalars1.  MT: type of mp (FP64, or FP32 when the
+// operator ran in FP32)
+template <typename MT>
 __global__ void __launch_bounds__(UT) k_msb_update_r(MsState* st, MsBlockVecs v, long n,
                                                      double* part) {
   if (st->skip) return;
@@ -430,7 +432,7 @@ __global__ void __launch_bounds__(UT) k_msb_update_r(MsState* st, MsBlockVecs v,
   double acc = 0.0;
   if (i < n) {
     double2 r = rin[i];
-    const double2 m = ((const double2*)v.mp)[i];
+    const MT m = ((const MT*)(sizeof(MT) == 16 ? v.mp : v.mp32))[i];
     r.x += b0 * m.x;
     r.y += b0 * m.y;
     rout[i] = r;
@@ -440,7 +442,7 @@ __global__ void __launch_bounds__(UT) k_msb_update_r(MsState* st, MsBlockVecs v,
   if (threadIdx.x == 0) part[blockIdx.x] = acc;
 }
 
-// p0 = r(i) + alpha_0 p0
+// p0 = r(i) + alpha_0 p0 (and its FP32 copy for an FP32 operator)
 __global__ void __launch_bounds__(UT) k_msb_update_p0(MsState* st, MsBlockVecs v, long n) {
   if (st->skip_b) return;
   const long i = (long)blockIdx.x * UT + threadIdx.x;
@@ -452,6 +454,50 @@ __global__ void __launch_bounds__(UT) k_msb_update_p0(MsState* st, MsBlockVecs v
   p.x = r.x + a0 * p.x;
   p.y = r.y + a0 * p.y;
   *pp = p;
+  if (v.p0_32) ((float2*)v.p0_32)[i] = make_float2((float)p.x, (float)p.y);
+}
+
+// Residual replacement at a block boundary (k = st->iter): r(k) becomes the
+// true residual rt, and the search vectors built from the old r(k) get the
+// same correction d = rt - r(k) so that p0 = r(k) + alpha p0_prev and
+// P_j = zeta_j r(k) + alpha_j P_j,prev keep holding (zeta_0 = 1)
+__global__ void __launch_bounds__(UT) k_msb_replace(MsState* st, MsBlockVecs v, long n,
+                                                    const double2* rt) {
+  __shared__ double z[MS_MAXS];
+  __shared__ int lv[MS_MAXS];
+  const int ns = st->nshift;
+  if (threadIdx.x < ns) {
+    const int j = threadIdx.x;
+    lv[j] = st->live[j];
+    z[j] = j == 0 ? 1.0 : st->zeta_i[j];
+  }
+  __syncthreads();
+  const long i = (long)blockIdx.x * UT + threadIdx.x;
+  if (i >= n) return;
+  double2* r = (double2*)v.ring[st->iter % (MS_BLK + 1)] + i;
+  const double2 t = rt[i];
+  const double2 d = make_double2(t.x - r->x, t.y - r->y);
+  *r = t;
+  double2* p0 = (double2*)v.p0 + i;
+  double2 p = *p0;
+  p.x += d.x;
+  p.y += d.y;
+  *p0 = p;
+  if (v.p0_32) ((float2*)v.p0_32)[i] = make_float2((float)p.x, (float)p.y);
+#pragma unroll 1
+  for (int j = 0; j < ns; j++) {
+    if (!lv[j]) continue;
+    double2* pj = (double2*)v.P[j] + i;
+    double2 q = *pj;
+    q.x += z[j] * d.x;
+    q.y += z[j] * d.y;
+    *pj = q;
+  }
+}
+
+__global__ void k_msb_set_rsq(MsState* st, double rsq) {
+  st->rsq = rsq;
+  st->skip = (rsq <= st->rsqstop || st->iter >= st->maxcg) ? 1 : 0;
 }
 
 // The block pass: every live shift's psi_j and P_j advanced over the
@@ -538,8 +584,21 @@ __global__ void k_msb_block_reset(MsState* st) {
   }
 }
 
-void msb_update_r(MsState* st, const MsBlockVecs& v, long n, double* part, cudaStream_t s) {
-  count_launch(), k_msb_update_r<<<vec_blocks(n), UT, 0, s>>>(st, v, n, part);
+void msb_update_r(MsState* st, const MsBlockVecs& v, long n, double* part, bool mp32,
+                  cudaStream_t s) {
+  if (mp32)
+    count_launch(), k_msb_update_r<float2><<<vec_blocks(n), UT, 0, s>>>(st, v, n, part);
+  else
+    count_launch(), k_msb_update_r<double2><<<vec_blocks(n), UT, 0, s>>>(st, v, n, part);
+}
+
+// Residual replacement: r(k) <- rt with the matching search-vector
+// correction, and the iterated |r|^2 becomes the true one (the stop flag
+// follows it)
+void msb_replace(MsState* st, const MsBlockVecs& v, long n, const void* rt, double rsq,
+                 cudaStream_t s) {
+  count_launch(), k_msb_replace<<<vec_blocks(n), UT, 0, s>>>(st, v, n, (const double2*)rt);
+  count_launch(), k_msb_set_rsq<<<1, 1, 0, s>>>(st, rsq);
 }
 
 void msb_update_p0(MsState* st, const MsBlockVecs& v, long n, cudaStream_t s) {

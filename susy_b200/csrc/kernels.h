@@ -42,12 +42,16 @@ struct MsVecs {
 // Vectors of the blocked solver: ring[i % (MS_BLK + 1)] holds the residual
 // after i iterations; P[j] is shift j's search vector at the block start
 // (P[0] a copy of the operator input p0 at that point); x[j] the solutions.
+// p0_32 / mp32: FP32 operator input and output when the operator runs in
+// FP32 (p0_32 written by the p0 update; nullptr in FP64).
 struct MsBlockVecs {
   void* ring[MS_BLK + 1];
   void* P[MS_MAXS];
   void* x[MS_MAXS];
   void* p0;
   void* mp;
+  void* p0_32;
+  void* mp32;
 };
 
 // fermion_op.cu, fermion_op_rows.cu
@@ -107,7 +111,10 @@ void ms_update_fused(MsState* st, const MsVecs& v, int prec, int prec_x, long n,
                      cudaStream_t s);
 void ms_update_p0(MsState* st, const MsVecs& v, int prec, long n, cudaStream_t s);
 void norm2_partials(const void* x, int prec, long n, double* part, cudaStream_t s);
-void msb_update_r(MsState* st, const MsBlockVecs& v, long n, double* part, cudaStream_t s);
+void msb_update_r(MsState* st, const MsBlockVecs& v, long n, double* part, bool mp32,
+                  cudaStream_t s);
+void msb_replace(MsState* st, const MsBlockVecs& v, long n, const void* rt, double rsq,
+                 cudaStream_t s);
 void msb_update_p0(MsState* st, const MsBlockVecs& v, long n, cudaStream_t s);
 void msb_block(MsState* st, const MsBlockVecs& v, long n, cudaStream_t s);
 

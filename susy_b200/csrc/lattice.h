@@ -36,6 +36,8 @@ struct susy_b200_lattice {
   std::vector<void*> pvec32;
   std::vector<void*> ring;    // residual ring of the blocked FP64 solver
   int ms_blocked = 1;         // FP64 multi-shift CG: blocked vector update
+  double mix_switch = 3e-4;   // mixed solver: FP32 operator once |r| < this |src|
+  double mix_reliable = 1e-2; // mixed solver: true residual when |r| fell this much
   std::vector<void*> extra;   // other lazily allocated fields
   int* poll = nullptr;        // pinned host words for solver polling
   // trajectory state (hmc.cu)

@@ -1,17 +1,19 @@
 // Host drivers of the device-resident solvers (cg.cu kernels).
 //
 // multishift_fp64   the reference's congrad_multi in FP64 throughout.
-// multishift_mixed  (1) the same multi-shift recurrences with the FP32
-//                   operator and FP32 search/residual vectors, solutions
-//                   accumulated in FP64, down to the FP32 noise floor;
-//                   (2) per shift, FP64 true residual r = b - (D^dag D +
-//                   sigma) x; while |r|^2 > errormin |b|^2, an FP32 CG on
-//                   (D^dag D + sigma) e = r (zero guess) and x += e in FP64
-//                   (defect correction with FP64 reliable updates).
-//                   Every shift ends at the same FP64 true residual bound
-//                   as the FP64 path requires.
+// multishift_mixed  (1) the same multi-shift recurrences (blocked update)
+//                   with the operator in FP32 once |r| < 3e-4 |src| and
+//                   FP64 reliable updates of the base residual;
+//                   (2) per shift, the FP64 true residual
+//                   r = b - (D^dag D + sigma) x; a shift with
+//                   |r|^2 > errormin |b|^2 gets an FP64 CG on
+//                   (D^dag D + sigma) e = r and x += e.
+//                   Every shift ends at or below the FP64 true residual
+//                   bound errormin |b|^2.
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <vector>
 #include "lattice.h"
 #include "hmc.h"
@@ -113,22 +115,47 @@ static void* ring_field(susy_b200_lattice* h, int q) {
   return h->ring[q];
 }
 
-// FP64 multi-shift CG with the blocked solution / search-vector update
+static void* refine_field(susy_b200_lattice* h, int i, int prec);
+static double true_residual(susy_b200_lattice* h, const void* b, const void* x, double sigma,
+                            void* r64, void* r32);
+
+// Multi-shift CG with the blocked solution / search-vector update
 // (cg.cu k_msb_block): the reference's recurrences and stopping rules,
 // the shifted vectors touched once per MS_BLK iterations.
+//
+// mixed = false: FP64 throughout (the reference's solver).
+// mixed = true: the operator runs in FP64 until |r| < mix_switch |src|
+// (handle setting, default 3e-4) and in FP32 after that; every vector,
+// the recurrences and the solutions stay FP64.  Once the operator is FP32,
+// the iterated residual drifts from the true one by the FP32 rounding of
+// each product, so at block boundaries, whenever |r| fell by mix_reliable
+// (default 1e-2) since the last check and when the solve stops, the FP64
+// true residual b - (D^dag D + sigma_0) psi_0 replaces it, with the same
+// correction applied to the search vectors (a reliable update); the solve
+// only ends when the true residual meets the stopping bound.  The FP32
+// products enter only when the residual is small, so the shifted systems,
+// which never see a residual replacement, keep an error of order FP32
+// rounding times that residual.  Switching earlier costs more in the
+// per-shift correction solves than it saves: measured at 12^3 x 24 U(3),
+// switching at 1e-3 took 894 iterations in all, at 3e-4 588 (FP64: 567).
+
 static int ms_run_block(susy_b200_lattice* h, const void* src, void* const* psim, int norder,
-                        const double* shift, int MaxCG, double errormin, double* size_r,
-                        int* iters) {
+                        const double* shift, int MaxCG, double errormin, bool mixed,
+                        double* size_r, int* iters) {
   cudaStream_t s = h->stream;
   const long n = tf_complex(h);
   const size_t bv = field_bytes(h, NTF, 64);
   void* p0 = scratch_tf(h, 3, 64);
   void* mp = scratch_tf(h, 5, 64);
   void* tmp = scratch_tf(h, 0, 64);
+  void* p0_32 = mixed ? scratch_tf(h, 3, 32) : nullptr;
+  void* mp32 = mixed ? scratch_tf(h, 5, 32) : nullptr;
+  void* tmp32 = mixed ? scratch_tf(h, 0, 32) : nullptr;
   double* part0 = partials(h, 0);
   double* part1 = partials(h, 1);
   int* pw = poll_words(h);
-  if (!p0 || !mp || !tmp || !part0 || !part1 || !pw) return set_err(h, SUSY_B200_ENOMEM);
+  if (!p0 || !mp || !tmp || !part0 || !part1 || !pw || (mixed && (!p0_32 || !mp32 || !tmp32)))
+    return set_err(h, SUSY_B200_ENOMEM);
   MsBlockVecs v;
   for (int q = 0; q <= MS_BLK; q++) {
     v.ring[q] = ring_field(h, q);
@@ -141,6 +168,8 @@ static int ms_run_block(susy_b200_lattice* h, const void* src, void* const* psim
   }
   v.p0 = p0;
   v.mp = mp;
+  v.p0_32 = nullptr;
+  v.mp32 = mp32;
   // r(0) = src, p0 = P_j = src, psi_j = 0   (congrad_multi.c:47-57)
   cudaMemcpyAsync(v.ring[0], src, bv, cudaMemcpyDeviceToDevice, s);
   cudaMemcpyAsync(p0, src, bv, cudaMemcpyDeviceToDevice, s);
@@ -157,21 +186,74 @@ static int ms_run_block(susy_b200_lattice* h, const void* src, void* const* psim
   const int np_vec = vec_blocks(n);
   const int* skip = &h->ms->skip;
   const int chunk = 2 * MS_BLK;
-  int launched = 0;
+  double* pd = (double*)(pw + 2);  // pinned: the iterated |r|^2
+  bool fp32_op = false;
+  double bnorm = 0.0, last_true = 0.0, rsqstop = 0.0;
+  if (mixed) {
+    cudaMemcpyAsync(pd, &h->ms->source_norm, sizeof(double), cudaMemcpyDeviceToHost, s);
+    if (!ck(h, cudaStreamSynchronize(s))) return SUSY_B200_ECUDA;
+    bnorm = last_true = *pd;
+    rsqstop = errormin * bnorm;
+  }
+  int launched = 0, replacements = 0;
+  // SUSY_B200_CG_TRACE=1 prints the solver's progress at every poll (stderr)
+  static const bool trace = [] {
+    const char* e = getenv("SUSY_B200_CG_TRACE");
+    return e && e[0] == '1';
+  }();
   for (;;) {
     for (int k = 0; k < chunk; k++) {
-      dev_fop(h, p0, tmp, 1, 64, nullptr, 0.0, nullptr, skip);
-      const int np_fop = dev_fop(h, tmp, mp, -1, 64, p0, fm2 + shift[0], part0, skip);
+      int np_fop;
+      if (fp32_op) {
+        dev_fop(h, p0_32, tmp32, 1, 32, nullptr, 0.0, nullptr, skip);
+        np_fop = dev_fop(h, tmp32, mp32, -1, 32, p0_32, fm2 + shift[0], part0, skip);
+      } else {
+        dev_fop(h, p0, tmp, 1, 64, nullptr, 0.0, nullptr, skip);
+        np_fop = dev_fop(h, tmp, mp, -1, 64, p0, fm2 + shift[0], part0, skip);
+      }
       ms_scalars1(h->ms, part0, np_fop, s);
-      msb_update_r(h->ms, v, n, part1, s);
+      msb_update_r(h->ms, v, n, part1, fp32_op, s);
       ms_scalars2(h->ms, part1, np_vec, s);
       msb_update_p0(h->ms, v, n, s);
       if ((k + 1) % MS_BLK == 0) msb_block(h->ms, v, n, s);
     }
     launched += chunk;
     cudaMemcpyAsync(pw, &h->ms->skip, sizeof(int), cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(pw + 1, &h->ms->iter, sizeof(int), cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(pd, &h->ms->rsq, sizeof(double), cudaMemcpyDeviceToHost, s);
     if (!ck(h, cudaStreamSynchronize(s))) return SUSY_B200_ECUDA;
-    if (pw[0] || launched >= MaxCG + chunk) break;
+    bool stop = pw[0] != 0;
+    if (trace)
+      fprintf(stderr, "susy_b200 cg: it %d rsq %.6e rel %.3e stop %d fp32 %d\n", pw[1], *pd,
+              bnorm > 0 ? *pd / bnorm : 0.0, (int)stop, (int)fp32_op);
+    if (mixed) {
+      const double rsq = *pd;
+      const int it = pw[1];
+      if (!fp32_op && !stop && rsq < h->mix_switch * h->mix_switch * bnorm) {
+        // the operator input from now on: an FP32 copy of p0, kept by the
+        // p0 update
+        fp32_op = true;
+        v.p0_32 = p0_32;
+        convert_field(n, p0, 64, p0_32, 32, s);
+      } else if (fp32_op && (stop || rsq < h->mix_reliable * h->mix_reliable * last_true)) {
+        // reliable update at the block boundary: psi_0 is current
+        void* rt64 = refine_field(h, 4, 64);
+        if (!rt64) return set_err(h, SUSY_B200_ENOMEM);
+        const double rt = true_residual(h, src, psim[0], shift[0], rt64, nullptr);
+        if (trace) fprintf(stderr, "susy_b200 cg: reliable update at %d: true rsq %.6e\n", it, rt);
+        if (!(rt == rt)) return set_err(h, SUSY_B200_ENAN);
+        msb_replace(h->ms, v, n, rt64, rt, s);
+        last_true = rt;
+        replacements++;
+        stop = (rt <= rsqstop || it >= MaxCG);
+      } else if (fp32_op && !(rsq <= 1e4 * last_true)) {
+        // the FP32 recurrence left the true residual behind: give up (the
+        // caller falls back to the FP64 solver)
+        if (trace) fprintf(stderr, "susy_b200 cg: FP32 phase diverged at %d\n", it);
+        return SUSY_B200_ENOCONV;
+      }
+    }
+    if (stop || launched >= MaxCG + chunk) break;
   }
   double rsq = 0.0;
   int it = 0;
@@ -189,7 +271,7 @@ int multishift_fp64(susy_b200_lattice* h, const void* src, void* const* psim, in
                     const double* shift, int MaxCG, double errormin, double* size_r,
                     int* iters) {
   if (h->ms_blocked)
-    return ms_run_block(h, src, psim, norder, shift, MaxCG, errormin, size_r, iters);
+    return ms_run_block(h, src, psim, norder, shift, MaxCG, errormin, false, size_r, iters);
   return ms_run(h, src, psim, norder, shift, MaxCG, errormin, 64, 64, size_r, iters);
 }
 
@@ -217,42 +299,43 @@ int multishift_mixed(susy_b200_lattice* h, const void* src, void* const* psim, i
                      const double* shift, int MaxCG, double errormin, double* size_r,
                      int* iters) {
   const long n = tf_complex(h);
-  void* src32 = refine_field(h, 0, 32);
-  void* r32 = refine_field(h, 1, 32);
-  void* e32 = refine_field(h, 3, 32);
-  if (!src32 || !r32 || !e32) return set_err(h, SUSY_B200_ENOMEM);
-  convert_field(n, src, 64, src32, 32, h->stream);
-  // (1) FP32 multi-shift pass; FP32 resolves |r|/|b| to ~1e-6
-  const double floor32 = 1e-12;
-  int it1 = 0, total = 0, rc;
+  int it1 = 0, rc;
   double sr = 0.0;
-  rc = ms_run(h, src32, psim, norder, shift, MaxCG, std::max(errormin, floor32), 32, 64, &sr,
-              &it1);
+  // (1) multi-shift pass, FP32 operator once the residual is small; should
+  // the FP32 phase fail (a non-finite value, or the iterated residual
+  // running away from the true one), the plain FP64 solve replaces it
+  rc = ms_run_block(h, src, psim, norder, shift, MaxCG, errormin, true, &sr, &it1);
+  if (rc == SUSY_B200_ENOCONV || rc == SUSY_B200_ENAN) {
+    cudaStreamSynchronize(h->stream);
+    h->err = 0;
+    int it64 = 0;
+    rc = ms_run_block(h, src, psim, norder, shift, MaxCG, errormin, false, &sr, &it64);
+    it1 += it64;
+  }
   if (rc) return rc;
-  total += it1;
-  // (2) FP64 true residuals and defect correction per shift
+  int total = it1;
+  // (2) every shift's FP64 true residual; a shift above the bound (the FP32
+  // products leave the shifted systems an error of order FP32 rounding
+  // times the residual at the switch) gets an FP64 correction solve
   double* part = partials(h, 2);
-  if (!part) return set_err(h, SUSY_B200_ENOMEM);
-  const double bnorm = [&] {
-    norm2_partials(src, 64, n, part, h->stream);
-    return host_sum(h, part, vec_blocks(n), 0);
-  }();
+  void* r64 = refine_field(h, 0, 64);
+  void* e64 = refine_field(h, 1, 64);
+  if (!part || !r64 || !e64) return set_err(h, SUSY_B200_ENOMEM);
+  norm2_partials(src, 64, n, part, h->stream);
+  const double bnorm = host_sum(h, part, vec_blocks(n), 0);
   const double target = errormin * bnorm;
   double worst = 0.0;
   for (int j = 0; j < norder; j++) {
-    double rr = true_residual(h, src, psim[j], shift[j], nullptr, r32);
-    for (int outer = 0; outer < 12 && rr > target; outer++) {
-      // inner FP32 CG to the remaining factor, capped at the FP32 floor
-      const double want = std::max(0.25 * target / rr, floor32);
-      void* e[1] = {e32};
+    double rr = true_residual(h, src, psim[j], shift[j], r64, nullptr);
+    for (int outer = 0; outer < 4 && rr > target && total < MaxCG; outer++) {
+      void* e[1] = {e64};
       int it2 = 0;
       double s2 = 0.0;
-      rc = ms_run(h, r32, e, 1, &shift[j], std::max(MaxCG - total, 1), want, 32, 32, &s2, &it2);
+      rc = ms_run(h, r64, e, 1, &shift[j], MaxCG - total, 0.25 * target / rr, 64, 64, &s2, &it2);
       if (rc) return rc;
       total += it2;
-      add_low(n, e32, psim[j], h->stream);
-      rr = true_residual(h, src, psim[j], shift[j], nullptr, r32);
-      if (total >= MaxCG) break;
+      axpy_field(n, 1.0, e64, psim[j], h->stream);
+      rr = true_residual(h, src, psim[j], shift[j], r64, nullptr);
     }
     worst = std::max(worst, rr);
   }

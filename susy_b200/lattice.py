@@ -126,6 +126,8 @@ def load_library(path: str = LIB_PATH):
     L.susy_b200_dev_DSq.argtypes = [_vp, _vp, _vp, C.c_int]
     L.susy_b200_autotune.argtypes = [_vp]
     L.susy_b200_fop_variant.argtypes = [_vp, C.c_int, C.c_int, C.POINTER(C.c_float)]
+    L.susy_b200_mixed_params.restype = C.c_int
+    L.susy_b200_mixed_params.argtypes = [_vp, C.c_double, C.c_double]
     L.susy_b200_cg_blocked.restype = C.c_int
     L.susy_b200_cg_blocked.argtypes = [_vp, C.c_int]
     L.susy_b200_dev_congrad_multi.argtypes = [_vp, _vp, C.POINTER(_vp), C.c_int, _dp, C.c_int,
@@ -383,6 +385,12 @@ class Lattice:
     # ---- operator kernel selection -----------------------------------------
     def autotune(self):
         self._check(self.lib.susy_b200_autotune(self.h))
+
+    def mixed_params(self, fp32_below: float = 3e-4, reliable_factor: float = 1e-2):
+        """Mixed solver: FP32 operator once |r| < fp32_below |src|; FP64
+        residual replacement whenever |r| fell by reliable_factor."""
+        self._check(self.lib.susy_b200_mixed_params(self.h, float(fp32_below),
+                                                    float(reliable_factor)))
 
     def cg_blocked(self, on: int = -1) -> int:
         """Blocked (1) or per-iteration (0) vector update of the FP64
