@@ -127,6 +127,35 @@ int susy_b200_dev_fermion_op(susy_b200_lattice *h, const void *src, void *dst, i
  * the fastest per precision; it also runs by itself on first use.
  * fop_variant returns the current variant of a precision, sets it when
  * set_to >= 0 and copies the autotuner's ms per variant when ms != NULL. */
+/* Per-trajectory measurements printed by control.c:85-138, on the
+ * handle's current links (and the derived fields of the last link update).
+ * Field by field the reference function and output line it reproduces. */
+typedef struct {
+  double linktr[5], linktr_ave, linktr_width;   /* link_trace.c:9, FLINK      */
+  double link_det[5], det_ave, det_width;       /* link_trace.c:9, FLINK_DET  */
+  double ploop_re, ploop_im, ploop_mod;         /* ploop(TUP, NODET), GMES    */
+  double ss_plaq, st_plaq;                      /* plaquette, plaq.c:7, GMES  */
+  double gauge_action;                          /* gauge_action(NODET),
+                                                   action.c:106; BACTION is
+                                                   this / volume             */
+  double lines_re[5], lines_im[5];              /* ploop(dir, NODET), LINES   */
+  double lines_polar_re[5], lines_polar_im[5];  /* ploop(dir, YESDET),
+                                                   LINES_POLAR                */
+  double det_tot_re, det_tot_im, det_sq_re, det_sq_im, det_wsq;
+                                                /* measure_det,
+                                                   determinant.c:92, DET      */
+  double width_plaq, width_det_re, width_det_im; /* widths.c:8, WIDTHS        */
+  double uubar_ave[4], uubar_width[4], uubar_min[4], uubar_max[4];
+                                                /* scalar_eig(NODET),
+                                                   scalar_eig.c:15, UUBAR_EIG */
+  double polar_ave[4], polar_width[4], polar_min[4], polar_max[4];
+                                                /* scalar_eig(YESDET),
+                                                   POLAR_EIG (first NCOL used) */
+} susy_b200_meas;
+int susy_b200_measure(susy_b200_lattice *h, susy_b200_meas *m);
+/* plaquette(double *ss_plaq, double *st_plaq), plaq.c:7 */
+int susy_b200_plaquette(susy_b200_lattice *h, double *ss_plaq, double *st_plaq);
+
 /* FP64 multi-shift CG vector update (no reference counterpart; the
  * reference's congrad_multi.c:109-150 updates psi_j and p_j of every live
  * shift every iteration).  on = 1 (default): one pass per 8 iterations

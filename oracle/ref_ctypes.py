@@ -213,6 +213,53 @@ class RefLattice:
         it = self.lib.ref_grsource(_ptr(out))
         return out, it
 
+    # per-trajectory measurements (control.c:85-138) ------------------------
+    def ploop(self, d: int, project: int):
+        out = np.zeros(3)
+        self.lib.ref_ploop(int(d), int(project), _ptr(out))
+        return complex(out[0], out[1]), out[2]
+
+    def link_trace(self):
+        L = self.lib
+        L.ref_link_trace.restype = C.c_double
+        lt, ld = np.zeros(5), np.zeros(5)
+        w, da, dw = C.c_double(), C.c_double(), C.c_double()
+        ave = L.ref_link_trace(_ptr(lt), C.byref(w), _ptr(ld), C.byref(da), C.byref(dw))
+        return {"linktr": lt, "linktr_ave": ave, "linktr_width": w.value, "link_det": ld,
+                "det_ave": da.value, "det_width": dw.value}
+
+    def scalar_eig(self, project: int):
+        n = self.ncol
+        a, w, mn, mx = np.zeros(n), np.zeros(n), np.zeros(n), np.zeros(n)
+        self.lib.ref_scalar_eig(int(project), _ptr(a), _ptr(w), _ptr(mn), _ptr(mx))
+        return a, w, mn, mx
+
+    def gauge_action(self, do_det: int = 0):
+        self.lib.ref_gauge_action.restype = C.c_double
+        return self.lib.ref_gauge_action(int(do_det))
+
+    def _printed(self, fn, tag):
+        self.log()
+        start = len(self.log())
+        fn()
+        for line in self.log()[start:].splitlines():
+            if line.startswith(tag + " "):
+                return np.array([float(x) for x in line.split()[1:]])
+        raise RuntimeError("no %s line" % tag)
+
+    def measure_det(self):
+        """DET line of measure_det (determinant.c:92-120): 5 numbers"""
+        return self._printed(self.lib.ref_measure_det, "DET")
+
+    def widths(self):
+        """WIDTHS line of widths (widths.c:8-71): 3 numbers"""
+        return self._printed(self.lib.ref_widths, "WIDTHS")
+
+    def plaquette(self):
+        ss, st = C.c_double(), C.c_double()
+        self.lib.ref_plaquette(C.byref(ss), C.byref(st))
+        return ss.value, st.value
+
     def update(self):
         return self.lib.ref_update()
 

@@ -263,6 +263,29 @@ int ref_update(void) { return update(); }
 
 void ref_plaquette(double *ss, double *st) { plaquette(ss, st); }
 
+/* Per-trajectory measurements of control.c:85-138 (the reference's own
+ * functions; measure_det and widths print their results to stdout) */
+void ref_ploop(int dir, int project, double *out) {
+  double mod = 0.0;
+  complex c = ploop(dir, project, &mod);
+  out[0] = c.real; out[1] = c.imag; out[2] = mod;
+}
+
+double ref_link_trace(double *linktr, double *width, double *link_det, double *det_ave,
+                      double *det_width) {
+  return link_trace(linktr, width, link_det, det_ave, det_width);
+}
+
+void ref_scalar_eig(int project, double *ave, double *width, double *mn, double *mx) {
+  scalar_eig(project, ave, width, mn, mx);
+}
+
+double ref_gauge_action(int do_det) { return gauge_action(do_det); }
+
+void ref_measure_det(void) { measure_det(); fflush(stdout); }
+
+void ref_widths(void) { widths(); fflush(stdout); }
+
 /* Scalar globals a caller may need to mirror */
 void ref_params(double *out) {
   out[0] = kappa; out[1] = bmass; out[2] = fmass; out[3] = kappa_u1;

@@ -20,7 +20,10 @@ reference project, ``4d_Q16/``):
 * actions, link update, site RNG, momenta, pseudofermions and the Omelyan
   HMC trajectory (susy/action.c:106-328, susy/update_o.c:20-282,
   susy/grsource.c:44-304, generic/ranstuff.c:22-63,
-  libraries/gaussrand.c:12-32).
+  libraries/gaussrand.c:12-32),
+* the per-trajectory measurements of susy/control.c:85-138 (plaq.c,
+  ploop.c, link_trace.c, determinant.c:92-120, widths.c, scalar_eig.c,
+  unit.c:52-98).
 
 Pinned against the reference itself: ``tests/test_oracle_golden.py`` checks
 this module against vectors produced by the unmodified reference code
@@ -938,6 +941,145 @@ def update(h: HMCState, srcs_in=None, mom_in=None):
 
 # ---------------------------------------------------------------------------
 # Layout conversion between the reference's AoS (node_index order) and here
+# ---------------------------------------------------------------------------
+# Per-trajectory measurements printed by control.c:85-138
+def link_trace(U):
+    """Tr[U Ubar]/N per direction, its average and width, and the real
+    determinant of the traceless part of U Ubar (link_trace.c:9-56)."""
+    N, V = U.shape[-1], U.shape[1]
+    M = U @ adj(U)
+    trs = np.real(tr(M))                                   # [5, V]
+    linktr = trs.sum(axis=1) / N / V
+    ave = float(linktr.mean())
+    sq = float((trs ** 2).sum()) / (N * N * V * NUMLINK)
+    T = M - (trs / N)[..., None, None] * np.eye(N)
+    dets = np.real(np.linalg.det(T))
+    link_det = dets.sum(axis=1) / V
+    det_ave = float(link_det.mean())
+    dsq = float((dets ** 2).sum()) / (V * NUMLINK)
+    return {"linktr": linktr, "linktr_ave": ave, "linktr_width": math.sqrt(sq - ave * ave),
+            "link_det": link_det, "det_ave": det_ave,
+            "det_width": math.sqrt(dsq - det_ave * det_ave)}
+
+
+def polar(U):
+    """U = P u with P = sqrt(U U^dag) Hermitian positive, u unitary
+    (unit.c:52-98); returns (u, P)."""
+    w, v = np.linalg.eigh(U @ adj(U))
+    P = (v * np.sqrt(w)[..., None, :]) @ adj(v)
+    Pinv = (v / np.sqrt(w)[..., None, :]) @ adj(v)
+    return Pinv @ U, P
+
+
+def ploop(geo: Geometry, U, d: int, project: int):
+    """Average trace of the product of links along direction d through the
+    whole lattice, from the sites with coordinate 0 along it (t for DIR_5),
+    and the average modulus (ploop.c:8-126).  project: polar-projected links."""
+    L = polar(U[d])[0] if project else U[d]
+    axis = d if d < 4 else 3
+    length = geo.dims[axis]
+    starts = np.nonzero(geo.coords[:, axis] == 0)[0]
+    cur = starts
+    prod = L[cur]
+    step = geo.nbr(OFFSETS[d])
+    for _ in range(1, length):
+        cur = step[cur]
+        prod = prod @ L[cur]
+    t = tr(prod)
+    norm = 1.0 / len(starts)
+    return complex(t.sum() * norm), float(np.abs(t).sum() * norm)
+
+
+def plaquette(geo: Geometry, U):
+    """Space-space and space-time plaquette averages (plaq.c:7-53):
+    Re Tr[U_a(x+b)^dag U_b(x)^dag U_a(x) U_b(x+a)] over b < a, the pairs with
+    the temporal link (a or b = 3) in st."""
+    ss = st = 0.0
+    for a in range(1, NUMLINK):
+        for b in range(a):
+            v = realtrace(geo.shift(U[a], b), adj(U[b]) @ U[a] @ geo.shift(U[b], a))
+            if a == 3 or b == 3:
+                st += v
+            else:
+                ss += v
+    return ss / (6.0 * geo.V), st / (4.0 * geo.V)
+
+
+def measure_det(geo: Geometry, der: Derived):
+    """DET line of measure_det (determinant.c:92-120)."""
+    tot = 0j
+    sq_re = sq_im = wsq = 0.0
+    for a in range(1, NUMLINK):
+        for b in range(a):
+            p = der.plaqdet[a, b]
+            tot += p.sum()
+            sq_re += float((p.real ** 2).sum())
+            sq_im += float((p.imag ** 2).sum())
+            wsq += float((np.abs(p - 1.0) ** 2).sum())
+    norm = 1.0 / (geo.V * NPLAQ)
+    return np.array([tot.real * norm, tot.imag * norm, sq_re * norm, sq_im * norm, wsq * norm])
+
+
+def widths(geo: Geometry, U):
+    """WIDTHS line (widths.c:8-71): widths of Re Tr P_ab and of the real and
+    imaginary parts of det P_ab, P_ab = U_b(x) U_a(x+b) [U_a(x) U_b(x+a)]^dag."""
+    acc = np.zeros(6)
+    for a in range(NUMLINK):
+        for b in range(a + 1, NUMLINK):
+            P = U[b] @ geo.shift(U[a], b) @ adj(U[a] @ geo.shift(U[b], a))
+            t = np.real(tr(P))
+            d = np.linalg.det(P)
+            acc += [t.sum(), (t ** 2).sum(), d.real.sum(), (d.real ** 2).sum(),
+                    d.imag.sum(), (d.imag ** 2).sum()]
+    acc *= 0.1 / geo.V
+    return np.array([math.sqrt(acc[1] - acc[0] ** 2), math.sqrt(acc[3] - acc[2] ** 2),
+                     math.sqrt(acc[5] - acc[4] ** 2)])
+
+
+def scalar_eig(U, project: int):
+    """Average, width, minimum and maximum of each (ascending) eigenvalue
+    over sites and links (scalar_eig.c:15-115): of the traceless part of
+    U Ubar, or (project) of log P from the polar decomposition, whose
+    eigenvalues are log(w)/2 for the eigenvalues w of U Ubar."""
+    N = U.shape[-1]
+    M = U @ adj(U)
+    if project:
+        e = 0.5 * np.log(np.linalg.eigvalsh(M))
+    else:
+        t = np.real(tr(M)) / N
+        e = np.linalg.eigvalsh(M - t[..., None, None] * np.eye(N))
+    e = e.reshape(-1, N)
+    ave = e.mean(axis=0)
+    width = np.sqrt((e ** 2).mean(axis=0) - ave ** 2)
+    return ave, width, e.min(axis=0), e.max(axis=0)
+
+
+def gauge_action(prm: Params, der: Derived):
+    """gauge_action(NODET) (action.c:106-142): kappa sum Re Tr[C2/2 D^2 +
+    2 sum F^dag F], C2 = 1."""
+    D, F = der.DmuUmu, der.Fmunu
+    t = 0.5 * np.real(tr(D @ D)).sum() + 2.0 * np.real(tr(adj(F) @ F)).sum()
+    return prm.kappa * float(t)
+
+
+def measurements(geo: Geometry, prm: Params, U, der: Derived):
+    """Every quantity control.c:85-138 prints after a trajectory."""
+    m = link_trace(U)
+    p, pm = ploop(geo, U, 3, 0)
+    m.update({"ploop_re": p.real, "ploop_im": p.imag, "ploop_mod": pm})
+    m["ss_plaq"], m["st_plaq"] = plaquette(geo, U)
+    m["gauge_action"] = gauge_action(prm, der)
+    lines = [ploop(geo, U, d, 0)[0] for d in range(NUMLINK)]
+    polar_lines = [ploop(geo, U, d, 1)[0] for d in range(NUMLINK)]
+    m["lines"] = np.array(lines)
+    m["lines_polar"] = np.array(polar_lines)
+    m["det"] = measure_det(geo, der)
+    m["widths"] = widths(geo, U)
+    m["uubar"] = scalar_eig(U, 0)
+    m["polar"] = scalar_eig(U, 1)
+    return m
+
+
 def tf_from_ref(geo: Geometry, flat: np.ndarray, N: int) -> np.ndarray:
     """Reference Twist_Fermion array (flat doubles) -> [16, V, N, N]."""
     a = flat.reshape(geo.V, 16, N, N, 2)

@@ -234,7 +234,7 @@ void susy_b200_destroy(susy_b200_lattice* h) {
   cudaStreamSynchronize(h->stream);
   void* ptrs[] = {h->U, h->mom, h->Uinv, h->force, h->det, h->pd, h->zw, h->D, h->F,
                   h->U32, h->Uinv32, h->pd32, h->stage, h->ms, h->bigpart, h->gen, h->prn,
-                  h->rng_bad, h->ptrbuf, h->nbrtab};
+                  h->rng_bad, h->ptrbuf, h->nbrtab, h->meas};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (int i = 0; i < SUSY_NSCRATCH; i++) {
@@ -253,6 +253,21 @@ void susy_b200_destroy(susy_b200_lattice* h) {
 }
 
 long long susy_b200_launch_count(void) { return g_launches.load(); }
+
+int susy_b200_measure(susy_b200_lattice* h, susy_b200_meas* m) {
+  if (!h || !m) return SUSY_B200_EINVAL;
+  return measure(h, m);
+}
+
+int susy_b200_plaquette(susy_b200_lattice* h, double* ss_plaq, double* st_plaq) {
+  if (!h || !ss_plaq || !st_plaq) return SUSY_B200_EINVAL;
+  susy_b200_meas m;
+  const int rc = measure(h, &m);
+  if (rc) return rc;
+  *ss_plaq = m.ss_plaq;
+  *st_plaq = m.st_plaq;
+  return SUSY_B200_OK;
+}
 
 int susy_b200_mixed_params(susy_b200_lattice* h, double fp32_below, double reliable_factor) {
   if (!h || !(fp32_below > 0.0 && fp32_below <= 1.0) ||

@@ -144,52 +144,7 @@ SUSY_D void mac(Mat<N, R>& acc, R s, const Mat<N, R>& A, const Mat<N, R>& B) {
     }
 }
 
-// FP32 accumulator for the operator kernels in packed-pair arithmetic
-// (two FP32 lanes per instruction, sm_100): P = sum a.re * b and
-// Q = sum a.im * b as (re, im) pairs, so a product a b = (P.x - Q.y,
-// P.y + Q.x) costs two pair-FMAs per complex multiply-add.
-template <int N>
-struct AccPair {
-  float2 P[N][N], Q[N][N];
-  SUSY_D void zero() {
-#pragma unroll
-    for (int i = 0; i < N; i++)
-#pragma unroll
-      for (int j = 0; j < N; j++) P[i][j] = Q[i][j] = make_float2(0.f, 0.f);
-  }
-  // += s * A B
-  SUSY_D void add(float s, const Mat<N, float>& A, const Mat<N, float>& B) {
-    float2 bs[N][N];
-    const float2 ss = make_float2(s, s);
-#pragma unroll
-    for (int k = 0; k < N; k++)
-#pragma unroll
-      for (int j = 0; j < N; j++) bs[k][j] = __fmul2_rn(make_float2(B.e[k][j].re, B.e[k][j].im), ss);
-#pragma unroll
-    for (int i = 0; i < N; i++)
-#pragma unroll
-      for (int k = 0; k < N; k++) {
-        const float2 ar = make_float2(A.e[i][k].re, A.e[i][k].re);
-        const float2 ai = make_float2(A.e[i][k].im, A.e[i][k].im);
-#pragma unroll
-        for (int j = 0; j < N; j++) {
-          P[i][j] = __ffma2_rn(ar, bs[k][j], P[i][j]);
-          Q[i][j] = __ffma2_rn(ai, bs[k][j], Q[i][j]);
-        }
-      }
-  }
-  SUSY_D Mat<N, float> get() const {
-    Mat<N, float> m;
-#pragma unroll
-    for (int i = 0; i < N; i++)
-#pragma unroll
-      for (int j = 0; j < N; j++)
-        m.e[i][j] = Cx<float>(P[i][j].x - Q[i][j].y, P[i][j].y + Q[i][j].x);
-    return m;
-  }
-};
-
-// Plain accumulator with the same interface (FP64)
+// Matrix accumulator of the table-driven operator kernels
 template <int N, typename R>
 struct AccMat {
   Mat<N, R> m;
@@ -197,9 +152,6 @@ struct AccMat {
   SUSY_D void add(R s, const Mat<N, R>& A, const Mat<N, R>& B) { mac<0>(m, s, A, B); }
   SUSY_D Mat<N, R> get() const { return m; }
 };
-
-template <int N, typename R> struct AccOf { typedef AccMat<N, R> T; };
-template <int N> struct AccOf<N, float> { typedef AccPair<N> T; };
 
 template <int N, typename R>
 SUSY_D void axpy(Mat<N, R>& acc, Cx<R> c, const Mat<N, R>& A) {

@@ -10,61 +10,11 @@
 // in place of the reference's LAPACK zgetrf/zgetri calls.
 #include "common.cuh"
 #include "kernels.h"
+#include "linalg.cuh"
 
 namespace susy {
 
 constexpr int DT = 128;
-
-template <int N>
-SUSY_D void det_inv(const Mat<N, double>& A, Cx<double>& det, Mat<N, double>& inv) {
-  Mat<N, double> a = A;
-  inv.zero();
-#pragma unroll
-  for (int i = 0; i < N; i++) inv.e[i][i] = Cx<double>(1, 0);
-  det = Cx<double>(1, 0);
-#pragma unroll
-  for (int k = 0; k < N; k++) {
-    int p = k;
-    double best = fabs(a.e[k][k].re) + fabs(a.e[k][k].im);
-#pragma unroll
-    for (int i = k + 1; i < N; i++) {
-      double v = fabs(a.e[i][k].re) + fabs(a.e[i][k].im);
-      if (v > best) { best = v; p = i; }
-    }
-    if (p != k) {
-      det = Cx<double>(-det.re, -det.im);
-#pragma unroll
-      for (int j = 0; j < N; j++) {
-        // swap rows k and p (register arrays indexed through a select)
-#pragma unroll
-        for (int i = k + 1; i < N; i++)
-          if (i == p) {
-            Cx<double> t = a.e[k][j]; a.e[k][j] = a.e[i][j]; a.e[i][j] = t;
-            t = inv.e[k][j]; inv.e[k][j] = inv.e[i][j]; inv.e[i][j] = t;
-          }
-      }
-    }
-    Cx<double> piv = a.e[k][k];
-    det = det * piv;
-    double d2 = piv.re * piv.re + piv.im * piv.im;
-    Cx<double> r(piv.re / d2, -piv.im / d2);
-#pragma unroll
-    for (int j = 0; j < N; j++) {
-      a.e[k][j] = a.e[k][j] * r;
-      inv.e[k][j] = inv.e[k][j] * r;
-    }
-#pragma unroll
-    for (int i = 0; i < N; i++) {
-      if (i == k) continue;
-      Cx<double> f = a.e[i][k];
-#pragma unroll
-      for (int j = 0; j < N; j++) {
-        a.e[i][j] = a.e[i][j] - f * a.e[k][j];
-        inv.e[i][j] = inv.e[i][j] - f * inv.e[k][j];
-      }
-    }
-  }
-}
 
 // det U_a(x) and U_a(x)^{-1} for every (site, link)
 template <int N>

@@ -335,8 +335,7 @@ fermion_op_compact_kernel(FopArgs<R> a) {
 // flight while the current one is multiplied, with no register copies
 // between iterations (a rolled loop with one prefetch buffer copies both
 // matrices every term).  Both block orders are built; which one wins
-// depends on the precision (the autotuner decides).  In FP32 the products
-// run in packed-pair arithmetic (AccPair, common.cuh).
+// depends on the precision (the autotuner decides).
 
 // Shared epilogue: determinant terms, adjoint for D^dag, axpy and dot
 template <int N, typename R, int SIGN>
@@ -412,8 +411,8 @@ SUSY_D void run_pattern_pp(ACC& acc, const FopArgs<R>& a, int s, unsigned bcm, i
   }
 }
 
-// Block order: site-major (SM = true) or component-major.  FP32 accumulates
-// in packed pairs (AccPair), FP64 in a plain matrix.
+// Block order: site-major (SM = true) or component-major; PP: two operand
+// buffers (prefetch) or one.
 template <int N, typename R, int SIGN, bool SM, bool PP>
 __global__ void __launch_bounds__(CT_THREADS)
 fermion_op_pp_kernel(FopArgs<R> a) {
@@ -424,7 +423,7 @@ fermion_op_pp_kernel(FopArgs<R> a) {
   if (s < a.g.V) {
     const Site c = site_of(a.g, s);
     const unsigned bcm = bc_mask(a.g, c);
-    typename AccOf<N, R>::T acc;
+    AccMat<N, R> acc;
     acc.zero();
     run_pattern_pp<N, R, SIGN, P_UF, PP>(acc, a, s, bcm, c_pat_start[comp][0], c_pat_start[comp][1]);
     run_pattern_pp<N, R, SIGN, P_FU, PP>(acc, a, s, bcm, c_pat_start[comp][1], c_pat_start[comp][2]);
@@ -487,9 +486,9 @@ int fermion_op_compact(const FopArgs<R>& a, int N, int sign, int variant, cudaSt
       }
     default:
       switch (N) {
-        case 2: return launch_pp<2, R, false, false>(a, sign, st);
-        case 3: return launch_pp<3, R, false, false>(a, sign, st);
-        default: return launch_pp<4, R, false, false>(a, sign, st);
+        case 2: return launch_pp<2, R, true, false>(a, sign, st);
+        case 3: return launch_pp<3, R, true, false>(a, sign, st);
+        default: return launch_pp<4, R, true, false>(a, sign, st);
       }
   }
 }

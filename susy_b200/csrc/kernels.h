@@ -61,12 +61,10 @@ struct MsBlockVecs {
 // FOP_COMPACT evaluates all 220 products from a constant-memory term table;
 // FOP_COMPACT_PF also prefetches the next product's operands.
 // FOP_SITE_MAJOR_PP / FOP_COMP_MAJOR_PP: table-driven with two alternating
-// operand buffers, site-major or component-major block order, FP32 in
-// packed-pair arithmetic; FOP_COMP_MAJOR_PAIR: the same component-major
-// kernel with one operand buffer (fewest registers).
+// operand buffers, site-major or component-major block order;
+// FOP_SITE_MAJOR: site-major with one operand buffer (fewest registers).
 enum { FOP_MAT = 0, FOP_MAT_CM = 1, FOP_ROWS = 2, FOP_COMPACT = 3, FOP_COMPACT_PF = 4,
-       FOP_SITE_MAJOR_PP = 5, FOP_COMP_MAJOR_PP = 6, FOP_COMP_MAJOR_PAIR = 7,
-       FOP_NVARIANTS = 8 };
+       FOP_SITE_MAJOR_PP = 5, FOP_COMP_MAJOR_PP = 6, FOP_SITE_MAJOR = 7, FOP_NVARIANTS = 8 };
 template <typename R>
 int fermion_op(const Geo& g, int N, const void* U, const void* Uinv, const void* pd,
                 const void* src, void* dst, int sign, double G, const void* add, double addc,

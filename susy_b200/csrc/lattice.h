@@ -35,6 +35,8 @@ struct susy_b200_lattice {
   std::vector<void*> pvec64;  // p_j of the FP64 multi-shift CG
   std::vector<void*> pvec32;
   std::vector<void*> ring;    // residual ring of the blocked FP64 solver
+  double* meas = nullptr;     // measurement partials
+  size_t meas_n = 0;
   int ms_blocked = 1;         // FP64 multi-shift CG: blocked vector update
   double mix_switch = 3e-4;   // mixed solver: FP32 operator once |r| < this |src|
   double mix_reliable = 1e-2; // mixed solver: true residual when |r| fell this much
@@ -73,4 +75,5 @@ void* sol_field(susy_b200_lattice* h, int j);
 int multishift_fp64(susy_b200_lattice* h, const void* src, void* const* psim, int norder,
                     const double* shift, int MaxCG, double errormin, double* size_r,
                     int* iters);
+int measure(susy_b200_lattice* h, susy_b200_meas* m);
 }  // namespace susy

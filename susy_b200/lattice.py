@@ -49,6 +49,26 @@ SOLVER_MIXED = 1
 FOP_NVARIANTS = 8
 
 
+class Meas(C.Structure):
+    """susy_b200_meas: the measurements of control.c:85-138."""
+    _fields_ = [("linktr", C.c_double * 5), ("linktr_ave", C.c_double),
+                ("linktr_width", C.c_double), ("link_det", C.c_double * 5),
+                ("det_ave", C.c_double), ("det_width", C.c_double),
+                ("ploop_re", C.c_double), ("ploop_im", C.c_double), ("ploop_mod", C.c_double),
+                ("ss_plaq", C.c_double), ("st_plaq", C.c_double),
+                ("gauge_action", C.c_double),
+                ("lines_re", C.c_double * 5), ("lines_im", C.c_double * 5),
+                ("lines_polar_re", C.c_double * 5), ("lines_polar_im", C.c_double * 5),
+                ("det_tot_re", C.c_double), ("det_tot_im", C.c_double),
+                ("det_sq_re", C.c_double), ("det_sq_im", C.c_double), ("det_wsq", C.c_double),
+                ("width_plaq", C.c_double), ("width_det_re", C.c_double),
+                ("width_det_im", C.c_double),
+                ("uubar_ave", C.c_double * 4), ("uubar_width", C.c_double * 4),
+                ("uubar_min", C.c_double * 4), ("uubar_max", C.c_double * 4),
+                ("polar_ave", C.c_double * 4), ("polar_width", C.c_double * 4),
+                ("polar_min", C.c_double * 4), ("polar_max", C.c_double * 4)]
+
+
 class RHMC:
     """Owns the coefficient arrays behind a RHMCParams structure."""
 
@@ -126,6 +146,10 @@ def load_library(path: str = LIB_PATH):
     L.susy_b200_dev_DSq.argtypes = [_vp, _vp, _vp, C.c_int]
     L.susy_b200_autotune.argtypes = [_vp]
     L.susy_b200_fop_variant.argtypes = [_vp, C.c_int, C.c_int, C.POINTER(C.c_float)]
+    L.susy_b200_measure.restype = C.c_int
+    L.susy_b200_measure.argtypes = [_vp, C.POINTER(Meas)]
+    L.susy_b200_plaquette.restype = C.c_int
+    L.susy_b200_plaquette.argtypes = [_vp, _dp, _dp]
     L.susy_b200_mixed_params.restype = C.c_int
     L.susy_b200_mixed_params.argtypes = [_vp, C.c_double, C.c_double]
     L.susy_b200_cg_blocked.restype = C.c_int
@@ -391,6 +415,34 @@ class Lattice:
         residual replacement whenever |r| fell by reliable_factor."""
         self._check(self.lib.susy_b200_mixed_params(self.h, float(fp32_below),
                                                     float(reliable_factor)))
+
+    def measure(self) -> dict:
+        """Measurements of control.c:85-138 on the current links, keyed as
+        the oracle's measurements()."""
+        m = Meas()
+        self._check(self.lib.susy_b200_measure(self.h, C.byref(m)))
+        n = self.N
+        a = lambda x, k=5: np.array(list(x)[:k])
+        return {"linktr": a(m.linktr), "linktr_ave": m.linktr_ave,
+                "linktr_width": m.linktr_width, "link_det": a(m.link_det),
+                "det_ave": m.det_ave, "det_width": m.det_width,
+                "ploop_re": m.ploop_re, "ploop_im": m.ploop_im, "ploop_mod": m.ploop_mod,
+                "ss_plaq": m.ss_plaq, "st_plaq": m.st_plaq, "gauge_action": m.gauge_action,
+                "lines": a(m.lines_re) + 1j * a(m.lines_im),
+                "lines_polar": a(m.lines_polar_re) + 1j * a(m.lines_polar_im),
+                "det": np.array([m.det_tot_re, m.det_tot_im, m.det_sq_re, m.det_sq_im,
+                                 m.det_wsq]),
+                "widths": np.array([m.width_plaq, m.width_det_re, m.width_det_im]),
+                "uubar": (a(m.uubar_ave, n), a(m.uubar_width, n), a(m.uubar_min, n),
+                          a(m.uubar_max, n)),
+                "polar": (a(m.polar_ave, n), a(m.polar_width, n), a(m.polar_min, n),
+                          a(m.polar_max, n))}
+
+    def plaquette(self):
+        """(ss_plaq, st_plaq), plaq.c:7"""
+        ss, st = C.c_double(), C.c_double()
+        self._check(self.lib.susy_b200_plaquette(self.h, C.byref(ss), C.byref(st)))
+        return ss.value, st.value
 
     def cg_blocked(self, on: int = -1) -> int:
         """Blocked (1) or per-iteration (0) vector update of the FP64

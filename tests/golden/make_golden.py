@@ -83,6 +83,23 @@ def ops_job(N, dims, seed):
     out["action_ampdeg4"] = ref.rhmc()["ampdeg4"]
     ref.ranmom()
     out["ranmom"] = ref.mom()
+    # per-trajectory measurements of control.c:85-138 on these links
+    ref.set_links(links)
+    ref.compute_all()
+    lt = ref.link_trace()
+    for k in ("linktr", "link_det"):
+        out["meas_" + k] = lt[k]
+    out["meas_lt_scalars"] = np.array([lt["linktr_ave"], lt["linktr_width"], lt["det_ave"],
+                                       lt["det_width"]])
+    pl = [ref.ploop(d, p) for p in (0, 1) for d in range(5)]
+    out["meas_lines"] = np.array([c for c, _ in pl])
+    out["meas_ploop_mod"] = pl[3][1]
+    out["meas_plaq"] = np.array(ref.plaquette())
+    out["meas_det"] = ref.measure_det()
+    out["meas_widths"] = ref.widths()
+    out["meas_uubar"] = np.array(ref.scalar_eig(0))
+    out["meas_polar"] = np.array(ref.scalar_eig(1))
+    out["meas_gauge_action"] = ref.gauge_action(0)
     return out
 
 
@@ -125,7 +142,34 @@ def parse_hmc_ref(path):
                           it_per_traj=int(its[k]),
                           monitor=[float(x) for x in mon[k]]))
     start = re.search(r"START (\S+) (\S+) (\S+) (\S+)", txt).groups()
-    return dict(trajectories=trajs, start_line=[float(x) for x in start])
+    # measurement lines (control.c:52-68 at start, :85-138 per trajectory)
+    nums = lambda line: [float(x) for x in line.split()[1:]]
+    lines = txt.splitlines()
+    meas, cur = [], None
+    start_meas = {}
+    for ln in lines:
+        tag = ln.split()[0] if ln.split() else ""
+        if tag in ("FLINK", "FLINK_DET") and not trajs_started(lines, ln):
+            start_meas[tag] = nums(ln)
+        if tag == "FLINK" and trajs_started(lines, ln):
+            cur = {}
+            meas.append(cur)
+        if cur is not None and tag in ("FLINK", "GMES", "BACTION", "LINES", "LINES_POLAR", "DET",
+                                       "WIDTHS"):
+            cur[tag] = nums(ln)
+        if cur is not None and tag in ("UUBAR_EIG", "POLAR_EIG"):
+            cur.setdefault(tag, []).append(nums(ln)[1:])
+    for k, m in enumerate(meas):
+        trajs[k]["meas"] = m
+    stop = re.search(r"STOP (\S+) (\S+) (\S+) (\S+)", txt)
+    return dict(trajectories=trajs, start_line=[float(x) for x in start], start_meas=start_meas,
+                stop_line=[float(x) for x in stop.groups()] if stop else None)
+
+
+def trajs_started(lines, line):
+    """True once the first trajectory's output precedes this line"""
+    i = lines.index(line)
+    return any(l.startswith("IT_PER_TRAJ") for l in lines[:i])
 
 
 def parse_input(path):

@@ -12,6 +12,8 @@ import os
 import numpy as np
 import pytest
 
+from measlines import mismatches, printed
+
 from susy_b200 import Lattice, RHMC, SOLVER_FP64, SOLVER_MIXED
 from susy_b200 import synth
 
@@ -88,7 +90,13 @@ def run_hmc_ref(N, solver):
              nstep_gauge=int(inp["nstep_gauge"]), traj_length=float(inp["traj_length"]),
              niter=int(inp["max_cg_iterations"]), error_per_site=float(inp["error_per_site"]),
              solver=solver)
-    return gold, [lat.update(r) for _ in gold["trajectories"]]
+    out = []
+    for _ in gold["trajectories"]:
+        t = lat.update(r)
+        t["meas"] = lat.measure()
+        t["V"] = lat.V
+        out.append(t)
+    return gold, out
 
 
 @pytest.mark.parametrize("N", [2, 3])
@@ -108,6 +116,12 @@ def test_cuda_reproduces_hmc_regression_output(N):
         assert g["max_gf"] == pytest.approx(t["monitor"][1], rel=2e-3)
         assert g["fnorm"][0] == pytest.approx(t["monitor"][2], rel=2e-3)
         assert g["max_ff"][0] == pytest.approx(t["monitor"][3], rel=2e-3)
+        # the measurement lines printed after the trajectory (control.c:85-138)
+        want = dict(t["meas"])
+        want["GMES"] = [x for k, x in enumerate(want["GMES"]) if k != 2]
+        got_lines = printed(g["meas"], g["V"])
+        got_lines["GMES"] = [x for k, x in enumerate(got_lines["GMES"]) if k != 2]
+        assert not mismatches(got_lines, want)
 
 
 def test_mixed_solver_keeps_the_accept_decisions():

@@ -133,3 +133,42 @@ def test_oracle_reproduces_hmc_U2_ref():
     assert abs(r["end"] - t0["end_S"]) < 1e-6
     assert abs(r["delta_S"] - t0["delta_S"]) < 1e-3 * max(abs(t0["delta_S"]), 1e-3)
     assert abs(r["iters"] - t0["it_per_traj"]) <= 12
+
+
+@pytest.mark.parametrize("N", [2, 3])
+def test_measurements(N):
+    """control.c:85-138 measurements of the oracle against the reference's
+    own functions on the same links (ops fixtures): link_trace, ploop in all
+    directions with and without polar projection, plaquette, scalar_eig and
+    gauge_action to 1e-12; measure_det and widths, which the reference only
+    prints (%.6g), to printed precision."""
+    d = load_ops(N)
+    dims, N, geo, prm, U, der = setup(d)
+    m = O.measurements(geo, prm, U, der)
+    assert rel(m["linktr"], d["meas_linktr"]) < 1e-12
+    assert rel(m["link_det"], d["meas_link_det"]) < 1e-12
+    assert rel(np.array([m["linktr_ave"], m["linktr_width"], m["det_ave"], m["det_width"]]),
+               d["meas_lt_scalars"]) < 1e-12
+    assert rel(np.concatenate([m["lines"], m["lines_polar"]]), d["meas_lines"]) < 1e-12
+    assert abs(m["ploop_mod"] - float(d["meas_ploop_mod"])) < 1e-12 * abs(m["ploop_mod"])
+    assert rel(np.array([m["ss_plaq"], m["st_plaq"]]), d["meas_plaq"]) < 1e-12
+    assert rel(np.array(m["uubar"]), d["meas_uubar"]) < 1e-12
+    assert rel(np.array(m["polar"]), d["meas_polar"]) < 1e-12
+    assert abs(m["gauge_action"] - float(d["meas_gauge_action"])) < 1e-12 * m["gauge_action"]
+    assert rel(m["det"], d["meas_det"]) < 3e-5
+    assert rel(m["widths"], d["meas_widths"]) < 3e-5
+
+
+@pytest.mark.parametrize("N", [2, 3])
+def test_measurements_on_the_regression_start_config(N):
+    """FLINK and FLINK_DET of the regression run's starting configuration
+    (testsuite/scalar/hmc.U{2,3}.ref, printed before the first trajectory)."""
+    from measlines import mismatches, printed
+    gold = json.load(open(os.path.join(GOLD, "hmc_U%d.json" % N)))
+    cfg = np.load(os.path.join(GOLD, "config_U%d_4444.npz" % N))
+    dims = tuple(int(x) for x in cfg["dims"])
+    geo = O.Geometry(dims, -1)
+    prm = O.Params(lam=float(gold["input"]["lambda"]), G=float(gold["input"]["G"]), N=N)
+    U = cfg["links"].astype(np.complex128)
+    m = O.measurements(geo, prm, U, O.compute_derived(geo, prm, U))
+    assert not mismatches(printed(m, geo.V), gold["start_meas"])
