@@ -247,6 +247,8 @@ int susy_b200_gaussian_tf(susy_b200_lattice *h, double *out);
 #define SUSY_B200_SOLVER_FP64 0    /* congrad_multi as the reference runs it   */
 #define SUSY_B200_SOLVER_MIXED 1   /* FP32 multi-shift + FP64 residual refinement */
 #define SUSY_B200_MAX_NROOT 4
+#define SUSY_B200_HMC 0            /* update_o.c:127 as built for susy_hmc      */
+#define SUSY_B200_SMD 1            /* the same with SMD_ALGORITHM (susy_smd)    */
 
 /* Rational approximation and integrator parameters: the reference globals
  * of susy/lattice.h:116-124 and setup_rhmc.c (amp4/shift4/amp8/shift8/
@@ -264,6 +266,15 @@ typedef struct {
   int no_metropolis;   /* 1: keep the end of every trajectory and only report
                           delta S, as the reference's non-HMC build does
                           (update_o.c:252-255) */
+  int algorithm;       /* SUSY_B200_HMC (0) or SUSY_B200_SMD */
+  double friction;     /* SMD friction (lattice.h:79, read at setup.c:324):
+                          momenta refreshed as mom <- c1 mom + c2 gaussian,
+                          c1 = exp(-traj_length friction) (0 if friction < 0),
+                          c1^2 + c2^2 = 1 (grsource.c:13-40); pseudofermion
+                          sources src <- c2 (fresh source) + c1 src with the
+                          reference's integer c1, c2 (grsource.c:74-197): a
+                          fresh source unless friction == 0, which keeps the
+                          previous trajectory's source */
 } susy_b200_rhmc;
 
 /* What update() prints (update_o.c:244-277) */
@@ -277,6 +288,10 @@ typedef struct {
 
 /* int grsource(Twist_Fermion *src)   susy/grsource.c:200; returns CG iterations */
 int susy_b200_grsource(susy_b200_lattice *h, const susy_b200_rhmc *r, double *src);
+/* void smdmom(Real eps)   susy/grsource.c:13 (friction passed explicitly):
+ * mom <- c1 mom + c2 (gaussian momenta as ranmom draws them),
+ * c1 = exp(-eps friction), 0 when friction < 0, c2 = sqrt(1 - c1^2) */
+int susy_b200_smdmom(susy_b200_lattice *h, double eps, double friction);
 /* int update()   susy/update_o.c:127: one HMC trajectory (momentum refresh,
  * pseudofermions, Omelyan integration, Metropolis with the node generator).
  * Returns the CG iteration count or a negative error code. */

@@ -13,6 +13,12 @@
 #   3. links oracle/_ref/n<NCOL>/susy_hmc (the reference program itself) and
 #      oracle/_ref/libsusyref_n<NCOL>.so (reference objects minus control.o,
 #      plus oracle/ref_harness.c) for ctypes.
+# An argument <NCOL>smd builds the same with -DSMD_ALGORITHM added
+# (the defines of susy/Make_template:112-116, target susy_smd) into
+# oracle/_ref/n<NCOL>smd/ and libsusyref_n<NCOL>_smd.so.  Not built by
+# default: that build's pseudofermion refresh reads uninitialised memory
+# (grsource.c:79-92) and printed NaN actions on its first trajectory here,
+# so it cannot serve as an oracle.
 # Outputs go only to oracle/_ref/ (git-ignored, shipped with the tree).
 # The reference's own build system is not used.
 set -euo pipefail
@@ -52,8 +58,11 @@ APP_FLAGS="-O3 -DP4 -Wall -fno-strict-aliasing -fPIC -DSINGLE -DPRECISION=2
 LIB_FLAGS="-O3 -Wall -fPIC -DPRECISION=2 -w"
 
 build_one() {
-  local N=$1
-  local D=$OUT/n$N
+  local N=${1%smd}
+  local ALG=-DHMC_ALGORITHM SUF=""
+  if [ "$1" != "$N" ]; then ALG="-DHMC_ALGORITHM -DSMD_ALGORITHM"; SUF=_smd; fi
+  local D=$OUT/n$1
+  local APP_FLAGS="${APP_FLAGS/-DHMC_ALGORITHM/$ALG}"
   mkdir -p "$D/obj"
   for sub in include susy generic libraries; do
     mkdir -p "$D/$sub"
@@ -100,9 +109,9 @@ build_one() {
   wait
 
   $CC -o "$D/susy_hmc" "$D/obj/control.o" "${objs[@]}" "$D/obj/lapack_min.o" -lm
-  $CC -shared -o "$OUT/libsusyref_n$N.so" "$D/obj/ref_harness.o" "${objs[@]}" \
+  $CC -shared -o "$OUT/libsusyref_n$N$SUF.so" "$D/obj/ref_harness.o" "${objs[@]}" \
       "$D/obj/lapack_min.o" -lm
-  echo "built $D/susy_hmc and $OUT/libsusyref_n$N.so"
+  echo "built $D/susy_hmc and $OUT/libsusyref_n$N$SUF.so"
 }
 
 mkdir -p "$OUT"

@@ -19,12 +19,12 @@ REF_DIR = os.path.join(HERE, "_ref")
 _dp = C.POINTER(C.c_double)
 
 
-def lib_path(ncol: int) -> str:
-    return os.path.join(REF_DIR, "libsusyref_n%d.so" % ncol)
+def lib_path(ncol: int, smd: bool = False) -> str:
+    return os.path.join(REF_DIR, "libsusyref_n%d%s.so" % (ncol, "_smd" if smd else ""))
 
 
-def available(ncol: int) -> bool:
-    return os.path.exists(lib_path(ncol))
+def available(ncol: int, smd: bool = False) -> bool:
+    return os.path.exists(lib_path(ncol, smd))
 
 
 def _ptr(a: np.ndarray):
@@ -34,14 +34,17 @@ def _ptr(a: np.ndarray):
 
 def input_text(dims, pbc=-1, iseed=41, Nroot=1, Norder=15, traj_length=1.0,
                nstep=5, nstep_gauge=4, lam=1.0, kappa_u1=0.0, bmass=0.0,
-               fmass=0.0, G=0.0, max_cg=5000, error_per_site=1e-5):
-    """Key/value input in the order setup.c:43-54,320-420 reads it."""
+               fmass=0.0, G=0.0, max_cg=5000, error_per_site=1e-5, friction=None):
+    """Key/value input in the order setup.c:43-54,320-420 reads it
+    (friction, setup.c:160-162, only for the SMD build)."""
     nx, ny, nz, nt = dims
     return "\n".join([
         "prompt 0", "nx %d" % nx, "ny %d" % ny, "nz %d" % nz, "nt %d" % nt,
         "PBC %d" % pbc, "iseed %d" % iseed, "Nroot %d" % Nroot,
         "Norder %d" % Norder, "warms 0", "trajecs 1",
-        "traj_length %.17g" % traj_length, "nstep %d" % nstep,
+        "traj_length %.17g" % traj_length] +
+        (["friction %.17g" % friction] if friction is not None else []) + [
+        "nstep %d" % nstep,
         "nstep_gauge %d" % nstep_gauge, "traj_between_meas 1",
         "lambda %.17g" % lam, "kappa_u1 %.17g" % kappa_u1,
         "bmass %.17g" % bmass, "fmass %.17g" % fmass, "G %.17g" % G,
@@ -52,9 +55,9 @@ def input_text(dims, pbc=-1, iseed=41, Nroot=1, Norder=15, traj_length=1.0,
 class RefLattice:
     """One reference lattice in this process."""
 
-    def __init__(self, ncol: int, quiet=True, **params):
+    def __init__(self, ncol: int, quiet=True, smd=False, **params):
         self.ncol = ncol
-        self.lib = C.CDLL(lib_path(ncol))
+        self.lib = C.CDLL(lib_path(ncol, smd))
         L = self.lib
         for name in ("ref_gauge_force", "ref_det_force", "ref_fermion_force",
                      "ref_update_gauge_step"):

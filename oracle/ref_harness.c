@@ -255,9 +255,14 @@ void ref_action_parts(double *src, double *sol, double *out) {
   free(ps);
 }
 
+#ifndef SMD_ALGORITHM
 void ref_ranmom(void) { ranmom(); }
 
 int ref_grsource(double *src) { return grsource((Twist_Fermion *)src); }
+#else
+/* The SMD build's refreshes (grsource.c:13-40,74-197) */
+void ref_smdmom(double eps) { smdmom(eps); }
+#endif
 
 int ref_update(void) { return update(); }
 

@@ -205,6 +205,22 @@ static void* field(susy_b200_lattice* h, std::vector<void*>& v, int i, int K) {
   return v[i];
 }
 
+// smdmom (grsource.c:13-40): mom <- c1 mom + c2 G, G drawn as ranmom draws
+// it from the per-site generators
+int dev_smdmom(susy_b200_lattice* h, double eps, double friction) {
+  const double c1 = friction < 0.0 ? 0.0 : std::exp(-eps * friction);
+  const double c2 = std::sqrt(1.0 - c1 * c1);
+  void* keep = field(h, h->extra5, 2, 5);
+  if (!keep) return SUSY_B200_ENOMEM;
+  const size_t b5 = field_bytes(h, 5, 64);
+  cudaMemcpyAsync(keep, h->mom, b5, cudaMemcpyDeviceToDevice, h->stream);
+  int rc = dev_ranmom(h);
+  if (rc) return rc;
+  scale_field(mat5(h), c2, h->mom, h->stream);
+  axpy_field(mat5(h), c1, keep, h->mom, h->stream);
+  return ck(h, cudaGetLastError()) ? SUSY_B200_OK : SUSY_B200_ECUDA;
+}
+
 // Solve with the configured solver; returns iterations (>= 0) or error
 int solve(susy_b200_lattice* h, const susy_b200_rhmc* r, const void* src, void* const* psim,
           const double* shifts) {
@@ -231,6 +247,26 @@ int dev_grsource(susy_b200_lattice* h, const susy_b200_rhmc* r, void* src, int* 
   const long n = 16L * h->N * h->N * h->g.S;
   scale_field(n, r->ampdeg8, src, h->stream);
   for (int j = 0; j < r->Norder; j++) axpy_field(n, r->amp8[j], ps[j], src, h->stream);
+  return ck(h, cudaGetLastError()) ? SUSY_B200_OK : SUSY_B200_ECUDA;
+}
+
+// smdgrsource (grsource.c:74-197): the fresh source of grsource, mixed
+// with the previous one as src <- c2 fresh + c1 src.  The reference holds
+// c1 and c2 in ints (grsource.c:79), so c1 = (int) exp(-traj_length
+// friction) is 1 for friction == 0 and 0 otherwise (0 also for friction <
+// 0), and c2 = (int) sqrt(1 - c1^2): the source is kept for friction == 0
+// and fresh for every other friction.  The gaussian draws and the shift8 CG
+// run either way, as in the reference.
+static int dev_smdgrsource(susy_b200_lattice* h, const susy_b200_rhmc* r, void* src, void* old,
+                           int* iters) {
+  const int c1 = r->friction < 0.0 ? 0 : (int)std::exp(-r->traj_length * r->friction);
+  const int c2 = (int)std::sqrt(1.0 - (double)(c1 * c1));
+  cudaMemcpyAsync(old, src, field_bytes(h, NTF, 64), cudaMemcpyDeviceToDevice, h->stream);
+  int rc = dev_grsource(h, r, src, iters);
+  if (rc) return rc;
+  const long n = 16L * h->N * h->N * h->g.S;
+  if (c2 != 1) scale_field(n, (double)c2, src, h->stream);
+  if (c1 != 0) axpy_field(n, (double)c1, old, src, h->stream);
   return ck(h, cudaGetLastError()) ? SUSY_B200_OK : SUSY_B200_ECUDA;
 }
 
@@ -280,7 +316,8 @@ static int gauge_step(susy_b200_lattice* h, const susy_b200_rhmc* r, double eps,
 
 int dev_update(susy_b200_lattice* h, const susy_b200_rhmc* r, susy_b200_traj* res,
                const double* mom_in, const double* const* src_in) {
-  if (r->Nroot < 1 || r->Nroot > SUSY_B200_MAX_NROOT || r->Norder < 1 || r->Norder > MS_MAXS)
+  if (r->Nroot < 1 || r->Nroot > SUSY_B200_MAX_NROOT || r->Norder < 1 || r->Norder > MS_MAXS ||
+      (r->algorithm != SUSY_B200_HMC && r->algorithm != SUSY_B200_SMD))
     return set_err(h, SUSY_B200_EINVAL);
   const int Nroot = r->Nroot, Norder = r->Norder;
   std::vector<void*> gsrc(Nroot);
@@ -298,11 +335,20 @@ int dev_update(susy_b200_lattice* h, const susy_b200_rhmc* r, susy_b200_traj* re
   memset(res, 0, sizeof(*res));
   int iters = 0, rc, it;
 
-  // ranmom (update_o.c:153) and pseudofermion sources (update_o.c:159-165)
-  if ((rc = dev_ranmom(h))) return rc;
+  // ranmom / smdmom (update_o.c:149-154) and pseudofermion sources
+  // (update_o.c:159-165)
+  const bool smd = r->algorithm == SUSY_B200_SMD;
+  if ((rc = smd ? dev_smdmom(h, r->traj_length, r->friction) : dev_ranmom(h))) return rc;
   if (mom_in && (rc = upload_links(h, h->mom, mom_in, 0, 5))) return rc;
   for (int n = 0; n < Nroot; n++) {
-    if ((rc = dev_grsource(h, r, gsrc[n], &it))) return rc;
+    if (smd) {
+      void* old = field(h, h->gsrc, SUSY_B200_MAX_NROOT + n, 16);
+      if (!old) return SUSY_B200_ENOMEM;
+      rc = dev_smdgrsource(h, r, gsrc[n], old, &it);
+    } else {
+      rc = dev_grsource(h, r, gsrc[n], &it);
+    }
+    if (rc) return rc;
     iters += it;
   }
   if (src_in)
@@ -467,6 +513,11 @@ int susy_b200_seed(susy_b200_lattice* h, int iseed) {
 int susy_b200_ranmom(susy_b200_lattice* h) {
   if (!h) return SUSY_B200_EINVAL;
   return dev_ranmom(h);
+}
+
+int susy_b200_smdmom(susy_b200_lattice* h, double eps, double friction) {
+  if (!h) return SUSY_B200_EINVAL;
+  return dev_smdmom(h, eps, friction);
 }
 
 int susy_b200_grsource(susy_b200_lattice* h, const susy_b200_rhmc* r, double* src) {

@@ -33,7 +33,7 @@ class RHMCParams(C.Structure):
                 ("amp8", _dp), ("shift8", _dp), ("ampdeg4", C.c_double),
                 ("ampdeg8", C.c_double), ("nsteps", C.c_int * 2), ("traj_length", C.c_double),
                 ("niter", C.c_int), ("rsqmin", C.c_double), ("solver", C.c_int),
-                ("no_metropolis", C.c_int)]
+                ("no_metropolis", C.c_int), ("algorithm", C.c_int), ("friction", C.c_double)]
 
 
 class TrajResult(C.Structure):
@@ -46,6 +46,8 @@ class TrajResult(C.Structure):
 
 SOLVER_FP64 = 0
 SOLVER_MIXED = 1
+HMC = 0
+SMD = 1
 FOP_NVARIANTS = 8
 
 
@@ -74,7 +76,7 @@ class RHMC:
 
     def __init__(self, Norder=15, Nroot=1, nstep=5, nstep_gauge=4, traj_length=1.0,
                  niter=5000, error_per_site=1e-5, solver=SOLVER_FP64, tables=None,
-                 no_metropolis=False):
+                 no_metropolis=False, algorithm=HMC, friction=0.0):
         if tables is None:
             from .rhmc_tables import rhmc
             tables = rhmc(Norder, Nroot)
@@ -94,6 +96,8 @@ class RHMC:
         self.p.rsqmin = error_per_site * error_per_site   # setup.c:356-359
         self.p.solver = solver
         self.p.no_metropolis = int(no_metropolis)
+        self.p.algorithm = int(algorithm)
+        self.p.friction = float(friction)
 
 
 class Params(C.Structure):
@@ -170,6 +174,8 @@ def load_library(path: str = LIB_PATH):
                                    C.c_double, _dp]
     L.susy_b200_seed.argtypes = [_vp, C.c_int]
     L.susy_b200_ranmom.argtypes = [_vp]
+    L.susy_b200_smdmom.restype = C.c_int
+    L.susy_b200_smdmom.argtypes = [_vp, C.c_double, C.c_double]
     L.susy_b200_gaussian_tf.argtypes = [_vp, _dp]
     L.susy_b200_grsource.argtypes = [_vp, C.POINTER(RHMCParams), _dp]
     L.susy_b200_update.argtypes = [_vp, C.POINTER(RHMCParams), C.POINTER(TrajResult)]
@@ -372,6 +378,10 @@ class Lattice:
 
     def ranmom(self):
         self._check(self.lib.susy_b200_ranmom(self.h))
+
+    def smdmom(self, eps: float, friction: float):
+        """smdmom(eps) (grsource.c:13): mom <- c1 mom + c2 gaussian"""
+        self._check(self.lib.susy_b200_smdmom(self.h, float(eps), float(friction)))
 
     def gaussian_tf(self) -> np.ndarray:
         out = np.zeros(self.tf_doubles)

@@ -77,7 +77,7 @@ def test_cuda_matches_reference_vectors(N):
     assert rel(lat.get_mom(), d["ranmom"]) < 1e-13
 
 
-def run_hmc_ref(N, solver):
+def run_hmc_ref(N, solver, **kw):
     gold = json.load(open(os.path.join(GOLD, "hmc_U%d.json" % N)))
     cfg = np.load(os.path.join(GOLD, "config_U%d_4444.npz" % N))
     inp = gold["input"]
@@ -89,7 +89,7 @@ def run_hmc_ref(N, solver):
     r = RHMC(int(inp["Norder"]), int(inp["Nroot"]), nstep=int(inp["nstep"]),
              nstep_gauge=int(inp["nstep_gauge"]), traj_length=float(inp["traj_length"]),
              niter=int(inp["max_cg_iterations"]), error_per_site=float(inp["error_per_site"]),
-             solver=solver)
+             solver=solver, **kw)
     out = []
     for _ in gold["trajectories"]:
         t = lat.update(r)
@@ -131,3 +131,17 @@ def test_mixed_solver_keeps_the_accept_decisions():
     for g, t in zip(got, gold["trajectories"]):
         assert g["accept"] == t["accept"]
         assert abs(g["delta_S"] - t["delta_S"]) <= 0.05
+
+
+def test_smd_with_full_refresh_is_the_hmc_regression_run():
+    """SMD (grsource.c:13-197, update_o.c SMD_ALGORITHM branches) with a
+    friction so large that c1 = exp(-traj_length friction) = 0 refreshes the
+    momenta completely (c2 = 1, the same gaussian draws as ranmom) and draws
+    fresh pseudofermion sources, which is the HMC trajectory: the three
+    trajectories of hmc.U2.ref come out again."""
+    from susy_b200 import SMD
+    gold, got = run_hmc_ref(2, SOLVER_FP64, algorithm=SMD, friction=1e300)
+    for g, t in zip(got, gold["trajectories"]):
+        assert g["accept"] == t["accept"]
+        assert abs(g["start"] - t["start_S"]) < 1e-6
+        assert abs(g["end"] - t["end_S"]) < 1e-6

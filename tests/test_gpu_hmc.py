@@ -213,3 +213,43 @@ def test_operator_variants_agree(N):
     assert all(abs(x[0] - solves[0][0]) <= 1 for x in solves), solves
     b2 = O.magsq(src)
     assert all(x[1] <= 1e-16 * b2 for x in solves), solves
+
+
+def test_smdmom_partial_refresh():
+    """smdmom (grsource.c:13-40): mom <- c1 mom + c2 G with G the momenta
+    ranmom would draw from the same generator state, c1 = exp(-eps friction),
+    c1^2 + c2^2 = 1; friction < 0 gives c1 = 0."""
+    import math
+    dims, N = (4, 4, 2, 4), 3
+    a, _, _, U = make(dims, N)
+    b, _, _, _ = make(dims, N)
+    mom0 = synth.to_ref(dims, synth.links(dims, N, 0.5, 9) - np.eye(N))
+    b.ranmom()
+    G = b.get_mom()
+    for eps, fr in ((0.7, 0.5), (1.0, -1.0)):
+        a.seed(41)
+        b.seed(41)
+        b.ranmom()
+        G = b.get_mom()
+        a.set_mom(mom0)
+        a.smdmom(eps, fr)
+        c1 = 0.0 if fr < 0 else math.exp(-eps * fr)
+        c2 = math.sqrt(1 - c1 * c1)
+        want = c1 * mom0 + c2 * G
+        assert np.abs(a.get_mom() - want).max() <= 1e-14 * np.abs(want).max()
+
+
+def test_smd_friction_zero_carries_the_momenta():
+    """friction 0: c1 = 1, c2 = 0, so the momenta enter the next trajectory
+    as the last one left them (negated after a rejection), and the integer
+    c1 of smdgrsource (grsource.c:79) keeps the pseudofermion source."""
+    from susy_b200 import SMD
+    dims, N = (4, 4, 4, 4), 2
+    lat, _, _, _ = make(dims, N, G=0.05, noise=0.05)
+    r0 = RHMC(15, 1, nstep=4, nstep_gauge=2, traj_length=0.5, error_per_site=1e-6,
+              algorithm=SMD, friction=0.0)
+    t1 = lat.update(r0)
+    m1 = lat.get_mom()
+    t2 = lat.update(r0)
+    # the start action's momentum term is that of the carried-over momenta
+    assert abs(t2["start_parts"][4] - float(np.dot(m1, m1))) <= 1e-9 * t2["start_parts"][4]
