@@ -402,6 +402,74 @@ def run_dsq_case(args):
                   flush=True)
 
 
+# Batched parameter scan of independent U(2) lattices: volumes from
+# {4^4, 6^4, 8^4, 4^3x8, 6^3x12, 8^3x16}, lambda from {0.5, 1, 2, 4}, link
+# noise 0.1-0.3, all seed-derived; bmass 0.2, G 0.05; degree-15 Nroot 1
+# rational approximation, 5 fermion steps x 4 gauge steps, error_per_site
+# 1e-5.
+BATCH_VOLS = [(4, 4, 4, 4), (6, 6, 6, 6), (8, 8, 8, 8), (4, 4, 4, 8), (6, 6, 6, 12),
+              (8, 8, 8, 16)]
+BATCH_LAMS = [0.5, 1.0, 2.0, 4.0]
+
+
+def run_batch_case(args):
+    """One RHMC trajectory on each of --lattices independent lattices,
+    concurrently (susy_b200_update_batch) and one after another, from the
+    same starting state: aggregate site-updates/s both ways (device time:
+    CUDA events on every lattice's stream, first start to last end) and the
+    largest |delta S| difference between a lattice batched and alone."""
+    import torch
+    from susy_b200 import Lattice, RHMC, synth, update_batch
+    rng = np.random.default_rng(2024)
+    lats, rhs, starts, streams = [], [], [], []
+    for i in range(args.lattices):
+        dims = BATCH_VOLS[int(rng.integers(len(BATCH_VOLS)))]
+        lam = float(rng.choice(BATCH_LAMS))
+        noise = float(rng.uniform(0.1, 0.3))
+        lat = Lattice(dims, 2, pbc=-1, lam=lam, bmass=0.2, G=0.05, iseed=1000 + i)
+        st = torch.cuda.Stream()
+        lat.set_stream(st.cuda_stream)
+        links = synth.to_ref(dims, synth.links(dims, 2, noise, 500 + i))
+        lats.append(lat)
+        streams.append(st)
+        starts.append(links)
+        rhs.append(RHMC(15, 1, nstep=5, nstep_gauge=4, traj_length=1.0, error_per_site=1e-5))
+
+    def reset():
+        for lat, links, i in zip(lats, starts, range(len(lats))):
+            lat.set_links(links)
+            lat.set_mom(np.zeros_like(links))
+            lat.seed(1000 + i)
+        torch.cuda.synchronize()
+
+    def timed(fn):
+        e0 = [torch.cuda.Event(enable_timing=True) for _ in lats]
+        e1 = [torch.cuda.Event(enable_timing=True) for _ in lats]
+        for e, st in zip(e0, streams):
+            e.record(st)
+        out = fn()
+        for e, st in zip(e1, streams):
+            e.record(st)
+        torch.cuda.synchronize()
+        return out, max(e0[0].elapsed_time(e) for e in e1)
+
+    update_batch(lats, rhs, args.threads)            # warm-up: allocation, autotune
+    reset()
+    batched, t_b = timed(lambda: update_batch(lats, rhs, args.threads))
+    reset()
+    alone, t_a = timed(lambda: [lat.update(r) for lat, r in zip(lats, rhs)])
+    sites = sum(lat.V for lat in lats)
+    dS = max(abs(b["delta_S"] - a["delta_S"]) for b, a in zip(batched, alone))
+    print(json.dumps({"case": "batched_lattices", "lattices": len(lats), "ncol": 2,
+                      "threads": args.threads, "total_sites": sites,
+                      "site_updates_per_s": sites / (t_b * 1e-3),
+                      "sequential_site_updates_per_s": sites / (t_a * 1e-3),
+                      "batched_ms": t_b, "sequential_ms": t_a, "speedup": t_a / t_b,
+                      "max_abs_delta_S_diff_vs_alone": dS,
+                      "accepted": sum(int(b["accept"]) for b in batched),
+                      "cg_iterations": sum(b["iters"] for b in batched)}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -414,9 +482,16 @@ def main():
     ap.add_argument("--dsq-case", action="store_true",
                     help="operator microbenchmark per kernel variant instead of the solve")
     ap.add_argument("--variant", type=int, default=-1)
+    ap.add_argument("--batch-case", action="store_true",
+                    help="independent U(2) lattices of uneven volume, batched vs one by one")
+    ap.add_argument("--lattices", type=int, default=48)
+    ap.add_argument("--threads", type=int, default=16)
     args = ap.parse_args()
     if args.dsq_case:
         run_dsq_case(args)
+        return
+    if args.batch_case:
+        run_batch_case(args)
         return
 
     world = int(os.environ.get("WORLD_SIZE", "1"))

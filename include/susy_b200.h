@@ -164,6 +164,12 @@ int susy_b200_plaquette(susy_b200_lattice *h, double *ss_plaq, double *st_plaq);
  * order); on = 0: the per-iteration update.  on < 0 only queries.
  * Returns the previous setting. */
 int susy_b200_cg_blocked(susy_b200_lattice *h, int on);
+/* Solver launch mode (no reference counterpart): on = 1 (default) captures
+ * the ~100 kernel launches of 16 solver iterations into a CUDA graph once
+ * per solve and operator precision and replays it; on = 0 launches them
+ * one by one.  Same kernels, same results.  on < 0 only queries; returns
+ * the previous setting. */
+int susy_b200_use_graphs(susy_b200_lattice *h, int on);
 /* Mixed-precision solver settings (no reference counterpart): the operator
  * runs in FP32 once |r| < fp32_below |src| (default 3e-4); with the FP32
  * operator the FP64 true residual replaces the iterated one whenever |r|
@@ -301,6 +307,14 @@ int susy_b200_update(susy_b200_lattice *h, const susy_b200_rhmc *r, susy_b200_tr
  * to replay a trajectory from known fields. */
 int susy_b200_update_replay(susy_b200_lattice *h, const susy_b200_rhmc *r, susy_b200_traj *res,
                             const double *mom, const double *const *src);
+
+/* Independent lattices at once (no reference counterpart: the reference
+ * runs one lattice per process): one update() per handle, h[i] with r[i]
+ * into res[i], the handles' streams driven concurrently by `threads` host
+ * threads.  Each lattice's result is the one update() gives it alone.
+ * Returns the total CG iterations or the first negative error code. */
+int susy_b200_update_batch(susy_b200_lattice *const *h, const susy_b200_rhmc *const *r,
+                           susy_b200_traj *res, int n, int threads);
 
 #ifdef __cplusplus
 }

@@ -17,6 +17,7 @@ namespace susy {
 
 static std::atomic<long long> g_launches(0);
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+void count_launches(long long n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
 static size_t mat_c(const susy_b200_lattice* h) { return (size_t)h->N * h->N; }
 
@@ -276,6 +277,13 @@ int susy_b200_mixed_params(susy_b200_lattice* h, double fp32_below, double relia
   h->mix_switch = fp32_below;
   h->mix_reliable = reliable_factor;
   return SUSY_B200_OK;
+}
+
+int susy_b200_use_graphs(susy_b200_lattice* h, int on) {
+  if (!h) return SUSY_B200_EINVAL;
+  const int prev = h->use_graphs;
+  if (on >= 0) h->use_graphs = on ? 1 : 0;
+  return prev;
 }
 
 int susy_b200_cg_blocked(susy_b200_lattice* h, int on) {

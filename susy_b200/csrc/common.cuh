@@ -23,6 +23,7 @@ namespace susy {
 // Host-side count of kernel launches made by this library (every launch
 // site is written as "count_launch(), kernel<<<...>>>(...)").
 void count_launch();
+void count_launches(long long n);
 
 constexpr int NUMLINK = 5;
 constexpr int NPLAQ = 10;

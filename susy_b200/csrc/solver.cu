@@ -115,6 +115,50 @@ static void* ring_field(susy_b200_lattice* h, int q) {
   return h->ring[q];
 }
 
+// One captured chunk of solver iterations.  Capture is thread-local, so
+// other host threads driving other lattices (susy_b200_update_batch) may
+// keep launching meanwhile.  If capture or instantiation fails the chunk
+// runs as plain launches.
+struct ChunkGraph {
+  cudaGraphExec_t exec = nullptr;
+  long long kernels = 0;
+  bool ready = false;
+  template <typename F>
+  void capture(susy_b200_lattice* h, int prec, F&& issue) {
+    // the operator's autotuner synchronises: run it before capturing
+    const int pi = prec == 64 ? 0 : 1;
+    if (h->fop_variant[pi] < 0) autotune_fop(h, prec);
+    cudaStream_t s = h->stream;
+    const long long c0 = susy_b200_launch_count();
+    if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+      cudaGetLastError();
+      h->use_graphs = 0;
+      return;
+    }
+    issue();
+    cudaGraph_t g = nullptr;
+    const cudaError_t e1 = cudaStreamEndCapture(s, &g);
+    kernels = susy_b200_launch_count() - c0;
+    count_launches(-kernels);   // captured, not launched
+    if (e1 != cudaSuccess || !g || cudaGraphInstantiate(&exec, g, 0) != cudaSuccess) {
+      cudaGetLastError();
+      if (g) cudaGraphDestroy(g);
+      exec = nullptr;
+      h->use_graphs = 0;
+      return;
+    }
+    cudaGraphDestroy(g);
+    ready = true;
+  }
+  void launch(cudaStream_t s) {
+    cudaGraphLaunch(exec, s);
+    count_launches(kernels);
+  }
+  ~ChunkGraph() {
+    if (exec) cudaGraphExecDestroy(exec);
+  }
+};
+
 static void* refine_field(susy_b200_lattice* h, int i, int prec);
 static double true_residual(susy_b200_lattice* h, const void* b, const void* x, double sigma,
                             void* r64, void* r32);
@@ -201,7 +245,7 @@ static int ms_run_block(susy_b200_lattice* h, const void* src, void* const* psim
     const char* e = getenv("SUSY_B200_CG_TRACE");
     return e && e[0] == '1';
   }();
-  for (;;) {
+  auto issue_chunk = [&]() {
     for (int k = 0; k < chunk; k++) {
       int np_fop;
       if (fp32_op) {
@@ -216,6 +260,22 @@ static int ms_run_block(susy_b200_lattice* h, const void* src, void* const* psim
       ms_scalars2(h->ms, part1, np_vec, s);
       msb_update_p0(h->ms, v, n, s);
       if ((k + 1) % MS_BLK == 0) msb_block(h->ms, v, n, s);
+    }
+  };
+  // A chunk's ~100 launches are captured once per operator precision into a
+  // CUDA graph and replayed: every argument of them is fixed for the solve
+  // (the convergence test and the freezing of shifts read device state).
+  ChunkGraph graphs[2];
+  for (;;) {
+    if (h->use_graphs) {
+      ChunkGraph& cg = graphs[fp32_op ? 1 : 0];
+      if (!cg.ready) cg.capture(h, fp32_op ? 32 : 64, issue_chunk);
+      if (cg.ready)
+        cg.launch(s);
+      else
+        issue_chunk();
+    } else {
+      issue_chunk();
     }
     launched += chunk;
     cudaMemcpyAsync(pw, &h->ms->skip, sizeof(int), cudaMemcpyDeviceToHost, s);

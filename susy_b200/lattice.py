@@ -156,6 +156,8 @@ def load_library(path: str = LIB_PATH):
     L.susy_b200_plaquette.argtypes = [_vp, _dp, _dp]
     L.susy_b200_mixed_params.restype = C.c_int
     L.susy_b200_mixed_params.argtypes = [_vp, C.c_double, C.c_double]
+    L.susy_b200_use_graphs.restype = C.c_int
+    L.susy_b200_use_graphs.argtypes = [_vp, C.c_int]
     L.susy_b200_cg_blocked.restype = C.c_int
     L.susy_b200_cg_blocked.argtypes = [_vp, C.c_int]
     L.susy_b200_dev_congrad_multi.argtypes = [_vp, _vp, C.POINTER(_vp), C.c_int, _dp, C.c_int,
@@ -174,6 +176,9 @@ def load_library(path: str = LIB_PATH):
                                    C.c_double, _dp]
     L.susy_b200_seed.argtypes = [_vp, C.c_int]
     L.susy_b200_ranmom.argtypes = [_vp]
+    L.susy_b200_update_batch.restype = C.c_int
+    L.susy_b200_update_batch.argtypes = [C.POINTER(_vp), C.POINTER(C.POINTER(RHMCParams)),
+                                         C.POINTER(TrajResult), C.c_int, C.c_int]
     L.susy_b200_smdmom.restype = C.c_int
     L.susy_b200_smdmom.argtypes = [_vp, C.c_double, C.c_double]
     L.susy_b200_gaussian_tf.argtypes = [_vp, _dp]
@@ -454,6 +459,11 @@ class Lattice:
         self._check(self.lib.susy_b200_plaquette(self.h, C.byref(ss), C.byref(st)))
         return ss.value, st.value
 
+    def use_graphs(self, on: int = -1) -> int:
+        """CUDA-graph replay (1) or plain launches (0) of the solver's
+        iteration chunks; returns the previous setting."""
+        return self._check(self.lib.susy_b200_use_graphs(self.h, int(on)))
+
     def cg_blocked(self, on: int = -1) -> int:
         """Blocked (1) or per-iteration (0) vector update of the FP64
         multi-shift CG; returns the previous setting (on < 0 only queries)."""
@@ -492,3 +502,18 @@ class Lattice:
         self._check(fn(self.h, src.ptr, arr, n, _ptr(shift), int(MaxCG), float(errormin),
                        C.byref(sr), C.byref(it)))
         return it.value, sr.value
+
+
+def update_batch(lattices, rhmcs, threads: int = 8):
+    """One trajectory on each lattice, concurrently (susy_b200_update_batch):
+    a list of the dicts Lattice.update returns."""
+    n = len(lattices)
+    assert len(rhmcs) == n and n > 0
+    lib = lattices[0].lib
+    hs = (_vp * n)(*[lat.h for lat in lattices])
+    rs = (C.POINTER(RHMCParams) * n)(*[C.pointer(r.p) for r in rhmcs])
+    res = (TrajResult * n)()
+    rc = lib.susy_b200_update_batch(hs, rs, res, n, int(threads))
+    if rc < 0:
+        lattices[0]._check(rc)
+    return [lat._traj(res[i]) for i, lat in enumerate(lattices)]

@@ -76,3 +76,24 @@ def test_blocked_update_matches_per_iteration(maxcg, errormin):
     assert abs(out[0][1] - out[1][1]) <= 1e-9 * out[0][1]
     for a, b in zip(out[0][2], out[1][2]):
         assert np.abs(a - b).max() <= 1e-11 * np.abs(a).max()
+
+
+@pytest.mark.parametrize("mixed", [False, True])
+def test_graph_replay_matches_plain_launches(mixed):
+    """The solver's iteration chunks replayed as CUDA graphs give the same
+    solve, bit for bit, as launching the kernels one by one."""
+    dims, N = (4, 4, 4, 8), 2
+    lat = Lattice(dims, N, pbc=-1, G=0.05)
+    lat.set_links(synth.to_ref(dims, synth.links(dims, N, 0.2, 4)))
+    src = lat.tf(64)
+    src.upload(synth.to_ref(dims, synth.tf_source(dims, N, seed=8)))
+    shifts = synth.geometric_shifts(15, 1e-5, 1e3)
+    out = {}
+    for on in (0, 1):
+        lat.use_graphs(on)
+        psim = [lat.tf(64) for _ in shifts]
+        it, rsq = lat.dev_congrad_multi(src, psim, shifts, 5000, 1e-20, mixed=mixed)
+        out[on] = (it, rsq, [p.download() for p in psim])
+    assert out[0][0] == out[1][0] and out[0][1] == out[1][1]
+    for a, b in zip(out[0][2], out[1][2]):
+        assert np.array_equal(a, b)

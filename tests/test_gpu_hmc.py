@@ -253,3 +253,29 @@ def test_smd_friction_zero_carries_the_momenta():
     t2 = lat.update(r0)
     # the start action's momentum term is that of the carried-over momenta
     assert abs(t2["start_parts"][4] - float(np.dot(m1, m1))) <= 1e-9 * t2["start_parts"][4]
+
+
+def test_update_batch_equals_one_by_one():
+    """susy_b200_update_batch: independent lattices of different volume and
+    NCOL run concurrently and each gets exactly the trajectory it gets alone."""
+    from susy_b200 import update_batch
+    specs = [((4, 4, 4, 4), 2, 0.1), ((4, 4, 2, 8), 2, 0.2), ((2, 4, 2, 4), 3, 0.15),
+             ((6, 6, 6, 6), 2, 0.3)]
+    def build():
+        out = []
+        for i, (dims, N, noise) in enumerate(specs):
+            lat = Lattice(dims, N, pbc=-1, lam=1.0 + i, bmass=0.2, G=0.05, iseed=7 + i)
+            lat.set_links(synth.to_ref(dims, synth.links(dims, N, noise, 30 + i)))
+            # a fixed kernel variant: the autotuner's pick depends on timing,
+            # which concurrency changes
+            lat.fop_variant(64, 3)
+            lat.fop_variant(32, 3)
+            out.append(lat)
+        return out
+    rh = [RHMC(15, 1, nstep=3, nstep_gauge=2, traj_length=0.5, error_per_site=1e-6)
+          for _ in specs]
+    got = update_batch(build(), rh, threads=4)
+    want = [lat.update(r) for lat, r in zip(build(), rh)]
+    for g, w in zip(got, want):
+        assert g["accept"] == w["accept"] and g["iters"] == w["iters"]
+        assert g["delta_S"] == w["delta_S"] and g["start"] == w["start"]
