@@ -308,6 +308,46 @@ int susy_b200_update(susy_b200_lattice *h, const susy_b200_rhmc *r, susy_b200_tr
 int susy_b200_update_replay(susy_b200_lattice *h, const susy_b200_rhmc *r, susy_b200_traj *res,
                             const double *mom, const double *const *src);
 
+/* ---- Learned preconditioner (no reference counterpart) ------------------
+ * A gauge-covariant network bound to a lattice handle (it reads the
+ * handle's current links): Twist_Fermion -> 16 site-type channels (each
+ * component's path closed with inverse links), three layers of
+ * parallel-transported nearest-neighbour convolutions 16 -> 32 -> 32 -> 16
+ * (11 taps: the site and both directions of the five links), back to a
+ * Twist_Fermion.  bfloat16 weights, FP32 arithmetic, FP64 device
+ * Twist_Fermions in and out.  Weights (susy_b200_net_nweights() complex
+ * numbers, re/im interleaved) are layer by layer W[tap][c_out][c_in]. */
+typedef struct susy_b200_net susy_b200_net;
+int susy_b200_net_nweights(void);
+susy_b200_net *susy_b200_net_create(susy_b200_lattice *h);
+void susy_b200_net_destroy(susy_b200_net *n);
+int susy_b200_net_set_weights(susy_b200_net *n, const double *w);
+int susy_b200_net_apply(susy_b200_net *n, const void *src, void *dst);
+/* loss = |N(r) - e|^2 / |e|^2 for device Twist_Fermions r, e; when grad is
+ * not NULL, grad += dL/dW* (complex interleaved, the layout of set_weights:
+ * dL/dRe w = 2 Re, dL/dIm w = 2 Im) */
+int susy_b200_net_loss_grad(susy_b200_net *n, const void *r, const void *e, double *loss,
+                            double *grad);
+/* The same with sigma >= 0: the A-norm error (d, A d) / (e, A e), d = N(r) - e,
+ * A = D^dag D + fmass^2 + sigma (e = A^-1 r, so (e, A e) = Re<e, r>);
+ * sigma < 0 is the plain relative error above. */
+int susy_b200_net_loss_grad2(susy_b200_net *n, const void *r, const void *e, double sigma,
+                             double *loss, double *grad);
+
+/* Multi-shift solve with learned preconditioning (config "FP32+learned"):
+ * the FP64 multi-shift stops the smallest (base) shift at loose |src|^2
+ * while the others freeze at errormin |src|^2 as usual; every shift whose
+ * FP64 true residual is still above errormin |src|^2 is then refined by
+ * flexible CG, preconditioned by net for the nrefine smallest shifts (net
+ * NULL: unpreconditioned).  Every shift ends at the FP64 true-residual
+ * bound.  iters: all operator applications (multi-shift iterations plus
+ * refinement iterations); refine_iters: the refinement part. */
+int susy_b200_dev_congrad_multi_learned(susy_b200_lattice *h, susy_b200_net *net,
+                                        const void *src, void *const *psim, int norder,
+                                        const double *shift, int MaxCG, double errormin,
+                                        int nrefine, double loose, double *size_r, int *iters,
+                                        int *refine_iters);
+
 /* Independent lattices at once (no reference counterpart: the reference
  * runs one lattice per process): one update() per handle, h[i] with r[i]
  * into res[i], the handles' streams driven concurrently by `threads` host

@@ -7,5 +7,7 @@ the reference interface (:class:`Lattice`) and seeded synthetic inputs.
 from .lattice import (Lattice, DeviceTF, SusyError, RHMC, load_library, LIB_PATH,  # noqa: F401
                       SOLVER_FP64, SOLVER_MIXED, HMC, SMD, update_batch)
 
-__all__ = ["Lattice", "DeviceTF", "SusyError", "RHMC", "load_library", "LIB_PATH",
+from . import learned  # noqa: F401,E402
+
+__all__ = ["learned", "Lattice", "DeviceTF", "SusyError", "RHMC", "load_library", "LIB_PATH",
            "SOLVER_FP64", "SOLVER_MIXED", "HMC", "SMD", "update_batch"]

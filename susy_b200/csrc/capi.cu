@@ -279,6 +279,18 @@ int susy_b200_mixed_params(susy_b200_lattice* h, double fp32_below, double relia
   return SUSY_B200_OK;
 }
 
+int susy_b200_dev_congrad_multi_learned(susy_b200_lattice* h, susy_b200_net* net,
+                                        const void* src, void* const* psim, int norder,
+                                        const double* shift, int MaxCG, double errormin,
+                                        int nrefine, double loose, double* size_r, int* iters,
+                                        int* refine_iters) {
+  if (!h || !src || !psim || !shift || norder < 1 || norder > MS_MAXS || nrefine < 0 ||
+      !(loose > 0.0))
+    return set_err(h, SUSY_B200_EINVAL);
+  return multishift_learned(h, net, src, psim, norder, shift, MaxCG, errormin, nrefine,
+                            loose < errormin ? errormin : loose, size_r, iters, refine_iters);
+}
+
 int susy_b200_use_graphs(susy_b200_lattice* h, int on) {
   if (!h) return SUSY_B200_EINVAL;
   const int prev = h->use_graphs;

@@ -42,6 +42,7 @@ __global__ void k_ms_init(MsState* st, const double* partials, int np, int maxcg
     st->source_norm = sn;
     st->rsq = sn;
     st->rsqstop = errormin * sn;
+    st->rsqfreeze = errormin * sn;
     st->iter = 0;
     st->maxcg = maxcg;
     for (int j = 0; j < st->nshift; j++) {
@@ -138,7 +139,7 @@ __global__ void k_ms_scalars2(MsState* st, const double* partials, int np) {
   st->rsq = rsqnew;
   for (int j = 1; j < st->nshift; j++) {
     if (st->converged[j]) continue;
-    if (rsqnew * st->zeta_ip1[j] * st->zeta_ip1[j] <= st->rsqstop) st->converged[j] = 1;
+    if (rsqnew * st->zeta_ip1[j] * st->zeta_ip1[j] <= st->rsqfreeze) st->converged[j] = 1;
   }
   for (int j = 0; j < st->nshift; j++) {
     if (st->converged[j]) continue;
@@ -495,6 +496,17 @@ __global__ void __launch_bounds__(UT) k_msb_replace(MsState* st, MsBlockVecs v, 
   }
 }
 
+// Stop the base system at errormin_base |src|^2 (shifts keep freezing at
+// rsqfreeze)
+__global__ void k_ms_set_stop(MsState* st, double errormin_base) {
+  st->rsqstop = errormin_base * st->source_norm;
+  st->skip = (st->rsq <= st->rsqstop || st->maxcg <= 0) ? 1 : 0;
+}
+
+void ms_set_stop(MsState* st, double errormin_base, cudaStream_t s) {
+  count_launch(), k_ms_set_stop<<<1, 1, 0, s>>>(st, errormin_base);
+}
+
 __global__ void k_msb_set_rsq(MsState* st, double rsq) {
   st->rsq = rsq;
   st->skip = (rsq <= st->rsqstop || st->iter >= st->maxcg) ? 1 : 0;
@@ -608,6 +620,28 @@ void msb_update_p0(MsState* st, const MsBlockVecs& v, long n, cudaStream_t s) {
 void msb_block(MsState* st, const MsBlockVecs& v, long n, cudaStream_t s) {
   count_launch(), k_msb_block<<<vec_blocks(n), UT, 0, s>>>(st, v, n);
   count_launch(), k_msb_block_reset<<<1, MS_MAXS, 0, s>>>(st);
+}
+
+// Re <a, b> partials over n FP64 complex entries
+__global__ void __launch_bounds__(UT) k_rdot(long n, const double2* a, const double2* b,
+                                             double* part) {
+  const long i = (long)blockIdx.x * UT + threadIdx.x;
+  double acc = 0.0;
+  if (i < n) {
+    const double2 u = a[i], v = b[i];
+    acc = u.x * v.x + u.y * v.y;
+  }
+  acc = block_sum<UT>(acc);
+  if (threadIdx.x == 0) part[blockIdx.x] = acc;
+}
+
+int rdot_partials(long n, const void* a, const void* b, double* part, cudaStream_t s) {
+  count_launch(), k_rdot<<<vec_blocks(n), UT, 0, s>>>(n, (const double2*)a, (const double2*)b, part);
+  return vec_blocks(n);
+}
+
+void copy_field(long n, const void* a, void* b, cudaStream_t s) {
+  cudaMemcpyAsync(b, a, (size_t)n * sizeof(double2), cudaMemcpyDeviceToDevice, s);
 }
 
 void norm2_partials(const void* x, int prec, long n, double* part, cudaStream_t s) {

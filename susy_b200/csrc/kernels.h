@@ -14,6 +14,8 @@ constexpr int MS_BLK = 8;
 // Device-resident state of one multi-shift solve (FP64 scalars)
 struct MsState {
   double rsq, rsqstop, source_norm, cd;
+  double rsqfreeze;   // shift j freezes once zeta_j^2 |r|^2 <= rsqfreeze (= rsqstop
+                      // unless a caller stops the base system earlier)
   int iter, maxcg, nshift, skip, skip_b, pad;
   // blocked update: per-iteration coefficients of the current block
   // (hb = beta_j, 0 once shift j is frozen; hz = zeta_j(i+1); ha = alpha_j),
@@ -109,12 +111,15 @@ void ms_update_fused(MsState* st, const MsVecs& v, int prec, int prec_x, long n,
                      cudaStream_t s);
 void ms_update_p0(MsState* st, const MsVecs& v, int prec, long n, cudaStream_t s);
 void norm2_partials(const void* x, int prec, long n, double* part, cudaStream_t s);
+int rdot_partials(long n, const void* a, const void* b, double* part, cudaStream_t s);
+void copy_field(long n, const void* a, void* b, cudaStream_t s);
 void msb_update_r(MsState* st, const MsBlockVecs& v, long n, double* part, bool mp32,
                   cudaStream_t s);
 void msb_replace(MsState* st, const MsBlockVecs& v, long n, const void* rt, double rsq,
                  cudaStream_t s);
 void msb_update_p0(MsState* st, const MsBlockVecs& v, long n, cudaStream_t s);
 void msb_block(MsState* st, const MsBlockVecs& v, long n, cudaStream_t s);
+void ms_set_stop(MsState* st, double errormin_base, cudaStream_t s);
 
 }  // namespace susy
 

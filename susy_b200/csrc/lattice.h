@@ -77,4 +77,9 @@ int multishift_fp64(susy_b200_lattice* h, const void* src, void* const* psim, in
                     const double* shift, int MaxCG, double errormin, double* size_r,
                     int* iters);
 int measure(susy_b200_lattice* h, susy_b200_meas* m);
+int net_apply(susy_b200_net* n, const void* src, void* dst);
+int multishift_learned(susy_b200_lattice* h, susy_b200_net* net, const void* src,
+                       void* const* psim, int norder, const double* shift, int MaxCG,
+                       double errormin, int nrefine, double loose, double* size_r, int* iters,
+                       int* refine_iters);
 }  // namespace susy

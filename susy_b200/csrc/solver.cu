@@ -185,7 +185,7 @@ static double true_residual(susy_b200_lattice* h, const void* b, const void* x, 
 
 static int ms_run_block(susy_b200_lattice* h, const void* src, void* const* psim, int norder,
                         const double* shift, int MaxCG, double errormin, bool mixed,
-                        double* size_r, int* iters) {
+                        double* size_r, int* iters, double errormin_base = -1.0) {
   cudaStream_t s = h->stream;
   const long n = tf_complex(h);
   const size_t bv = field_bytes(h, NTF, 64);
@@ -225,6 +225,7 @@ static int ms_run_block(susy_b200_lattice* h, const void* src, void* const* psim
   cudaMemcpyAsync(&h->ms->nshift, &ns, sizeof(int), cudaMemcpyHostToDevice, s);
   cudaMemcpyAsync(h->ms->shift, shift, sizeof(double) * norder, cudaMemcpyHostToDevice, s);
   ms_init(h->ms, src, 64, n, part0, MaxCG, errormin, s, 1);
+  if (errormin_base > 0.0) ms_set_stop(h->ms, errormin_base, s);
 
   const double fm2 = h->prm.fmass > 1e-8 ? h->prm.fmass * h->prm.fmass : 0.0;
   const int np_vec = vec_blocks(n);
@@ -403,6 +404,108 @@ int multishift_mixed(susy_b200_lattice* h, const void* src, void* const* psim, i
   if (!(worst == worst)) return set_err(h, SUSY_B200_ENAN);
   if (size_r) *size_r = worst;
   if (iters) *iters = total;
+  return SUSY_B200_OK;
+}
+
+// Flexible CG (Notay's FCG with one previous direction) on
+// (D^dag D + fmass^2 + sigma) x = b from the given x, preconditioned by the
+// network (identity when net is null: then it is plain CG), in FP64, until
+// |r|^2 <= target:
+//   z = M(r); p = z - (<z, q_prev> / <p_prev, q_prev>) p_prev; q = A p;
+//   alpha = <p, r> / <p, q>; x += alpha p; r -= alpha q.
+// The recursive residual is checked against the true one at the end (and
+// the iteration restarted from it once if the two disagree).
+static int fcg_refine(susy_b200_lattice* h, susy_b200_net* net, const void* b, void* x,
+                      double sigma, double target, int maxit, int* its) {
+  cudaStream_t s = h->stream;
+  const long n = tf_complex(h);
+  const double fm2 = h->prm.fmass > 1e-8 ? h->prm.fmass * h->prm.fmass : 0.0;
+  void* r = refine_field(h, 5, 64);
+  void* z = refine_field(h, 6, 64);
+  void* p = refine_field(h, 7, 64);
+  void* q = refine_field(h, 8, 64);
+  void* t = scratch_tf(h, 0, 64);
+  double* part = partials(h, 2);
+  if (!r || !z || !p || !q || !t || !part) return set_err(h, SUSY_B200_ENOMEM);
+  const int nb = vec_blocks(n);
+  auto dot = [&](const void* a, const void* c) {
+    rdot_partials(n, a, c, part, s);
+    return host_sum(h, part, nb, 0);
+  };
+  auto apply_A = [&](const void* in, void* out) {
+    dev_fop(h, in, t, 1, 64, nullptr, 0.0, nullptr, nullptr);
+    dev_fop(h, t, out, -1, 64, in, fm2 + sigma, nullptr, nullptr);
+  };
+  auto precond = [&](const void* in, void* out) -> int {
+    if (net) return net_apply(net, in, out);
+    copy_field(n, in, out, s);
+    return SUSY_B200_OK;
+  };
+  int it = 0, rc;
+  for (int restart = 0; restart < 2; restart++) {
+    double rr = true_residual(h, b, x, sigma, r, nullptr);
+    if (!(rr == rr)) return set_err(h, SUSY_B200_ENAN);
+    if (rr <= target) break;
+    if ((rc = precond(r, z))) return rc;
+    copy_field(n, z, p, s);
+    apply_A(p, q);
+    while (it < maxit) {
+      const double pq = dot(p, q);
+      const double alpha = dot(p, r) / pq;
+      axpy_field(n, alpha, p, x, s);
+      axpy_field(n, -alpha, q, r, s);
+      it++;
+      norm2_partials(r, 64, n, part, s);
+      rr = host_sum(h, part, nb, 0);
+      if (!(rr == rr)) return set_err(h, SUSY_B200_ENAN);
+      if (rr <= target) break;
+      if ((rc = precond(r, z))) return rc;
+      const double beta = -dot(z, q) / pq;
+      scale_field(n, beta, p, s);
+      axpy_field(n, 1.0, z, p, s);
+      apply_A(p, q);
+    }
+    if (it >= maxit) break;
+  }
+  if (its) *its = it;
+  return ck(h, cudaGetLastError()) ? SUSY_B200_OK : SUSY_B200_ECUDA;
+}
+
+// Learned-preconditioned solve: the blocked FP64 multi-shift with the base
+// (smallest) shift stopped at loose |src|^2 while the others keep freezing
+// at errormin |src|^2; then every shift whose FP64 true residual is above
+// errormin |src|^2 is refined by flexible CG, preconditioned by the network
+// for the nrefine smallest shifts and unpreconditioned for the rest.
+int multishift_learned(susy_b200_lattice* h, susy_b200_net* net, const void* src,
+                       void* const* psim, int norder, const double* shift, int MaxCG,
+                       double errormin, int nrefine, double loose, double* size_r, int* iters,
+                       int* refine_iters) {
+  int it1 = 0, rc;
+  double sr = 0.0;
+  rc = ms_run_block(h, src, psim, norder, shift, MaxCG, errormin, false, &sr, &it1, loose);
+  if (rc) return rc;
+  const long n = tf_complex(h);
+  double* part = partials(h, 2);
+  if (!part) return set_err(h, SUSY_B200_ENOMEM);
+  norm2_partials(src, 64, n, part, h->stream);
+  const double target = errormin * host_sum(h, part, vec_blocks(n), 0);
+  int total = it1, refine = 0;
+  double worst = 0.0;
+  void* r64 = refine_field(h, 0, 64);
+  if (!r64) return set_err(h, SUSY_B200_ENOMEM);
+  for (int j = 0; j < norder; j++) {
+    int its = 0;
+    rc = fcg_refine(h, j < nrefine ? net : nullptr, src, psim[j], shift[j], target,
+                    std::max(MaxCG - total, 1), &its);
+    if (rc) return rc;
+    total += its;
+    refine += its;
+    worst = std::max(worst, true_residual(h, src, psim[j], shift[j], r64, nullptr));
+  }
+  if (!(worst == worst)) return set_err(h, SUSY_B200_ENAN);
+  if (size_r) *size_r = worst;
+  if (iters) *iters = total;
+  if (refine_iters) *refine_iters = refine;
   return SUSY_B200_OK;
 }
 
