@@ -10,7 +10,13 @@ such solve.  Inputs are resident in HBM when the timed region starts; the
 working set (~3 GB) is larger than L2, so no flush is needed.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--solver fp64|mixed]
+                  [--solver mixed|fp64]
+
+The timed solver is the mixed one by default (FP64 operator until
+|r| < 3e-4 |src|, FP32 operator after, FP64 residual replacement and
+per-shift FP64 check: the same FP64 true-residual bound as the FP64 solver,
+reported as true_residual_rel_max); the FP64 solver of the reference's
+recurrences is timed right after it in the same run (fp64_s_per_solve).
 
 N > 1 runs one independent replica per GPU (torchrun, NCCL only for the
 barrier and the max-over-ranks time): "value" is the whole-job seconds per
@@ -234,8 +240,9 @@ def run_ours(args, rank, world, device):
     lat.autotune()
     mixed = args.solver == "mixed"
 
-    def solve():
-        return lat.dev_congrad_multi(src, psim, shifts, MAXCG, ERRORMIN, mixed=mixed)
+    def solve(m=None):
+        return lat.dev_congrad_multi(src, psim, shifts, MAXCG, ERRORMIN,
+                                     mixed=mixed if m is None else m)
 
     def barrier():
         if world > 1:
@@ -261,6 +268,23 @@ def run_ours(args, rank, world, device):
     barrier()
     torch.cuda.synchronize(device)
     ms_max = max_over_ranks(e0.elapsed_time(e1))
+    # the other solver on the same input, timed the same way (after one
+    # warm-up solve), for the FP32-vs-FP64 comparison of the metric
+    other = not mixed
+    solve(other)
+    lat.sync()
+    barrier()
+    torch.cuda.synchronize(device)
+    o0 = torch.cuda.Event(enable_timing=True)
+    o1 = torch.cuda.Event(enable_timing=True)
+    o0.record(st)
+    other_iters = 0
+    for _ in range(args.steps):
+        other_iters = solve(other)[0]
+    o1.record(st)
+    o1.synchronize()
+    other_ms = max_over_ranks(o0.elapsed_time(o1))
+    solve()                     # leave the timed solver's solutions in psim
     # FP64 true residual of every shift of the last solve, relative to |src|^2
     # (the stopping bound is 1e-20): checked on the host from the downloaded
     # solutions and their D^dag D
@@ -288,6 +312,15 @@ def run_ours(args, rank, world, device):
     f1.record(st)
     f1.synchronize()
     fop_ms = f0.elapsed_time(f1) / (2 * reps)
+    a32, b32 = lat.tf(32), lat.tf(32)
+    lat.dev_convert(a, a32)
+    lat.dev_DSq(a32, b32)
+    f0.record(st)
+    for _ in range(reps):
+        lat.dev_DSq(a32, b32)
+    f1.record(st)
+    f1.synchronize()
+    fop32_ms = f0.elapsed_time(f1) / (2 * reps)
     V = lat.V
     algo = algorithmic_bytes_fop(V, NCOL, 16)
     achieved = algo / (fop_ms * 1e-3) / 1e9
@@ -304,6 +337,7 @@ def run_ours(args, rank, world, device):
     h2d = d2h = 0
     if not args.no_e2e:
         import torch as _t
+        lat.set_solver(1 if mixed else 0)
         host_src = _t.empty(lat.tf_doubles, dtype=_t.float64, pin_memory=True).numpy()
         host_src[:] = src_host
         outs = [_t.empty(lat.tf_doubles, dtype=_t.float64, pin_memory=True).numpy()
@@ -336,12 +370,20 @@ def run_ours(args, rank, world, device):
                        "l2": "working set ~3 GB > 126 MB L2; no flush",
                        "iterations_per_solve": iters[-1],
                        "true_residual_rel_max": max(true_rel),
+                       ("fp64" if mixed else "mixed") + "_s_per_solve":
+                           seconds_per_solve(other_ms, args.steps, world),
+                       ("fp64" if mixed else "mixed") + "_iterations": other_iters,
+                       "speedup_vs_fp64": (other_ms / ms_max) if mixed else 1.0,
                        "fop_variant": lat.fop_variant(64)[0]},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak,
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": traffic, "kernel": "fermion_op (FP64, in DSq)",
                          "algorithmic_bytes_per_launch": algo, "launch_ms": fop_ms,
-                         "fp64_tflops": flops_fop(V, NCOL) / (fop_ms * 1e-3) / 1e12},
+                         "fp64_tflops": flops_fop(V, NCOL) / (fop_ms * 1e-3) / 1e12,
+                         "fp32_launch_ms": fop32_ms,
+                         "fp32_achieved": algorithmic_bytes_fop(V, NCOL, 8) / (fop32_ms * 1e-3) / 1e9,
+                         "fp32_frac": algorithmic_bytes_fop(V, NCOL, 8) / (fop32_ms * 1e-3) / 1e9 / peak,
+                         "fp32_variant": lat.fop_variant(32)[0]},
             "clocks": clk.summary(),
             "gpu_launches": launches,
             "e2e": {"value": seconds_per_solve(e2e_ms, args.steps, world) if e2e_ms else None,
@@ -476,7 +518,7 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--solver", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--solver", default="mixed", choices=["fp64", "mixed"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--dsq-case", action="store_true",

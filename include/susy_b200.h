@@ -170,6 +170,11 @@ int susy_b200_cg_blocked(susy_b200_lattice *h, int on);
  * one by one.  Same kernels, same results.  on < 0 only queries; returns
  * the previous setting. */
 int susy_b200_use_graphs(susy_b200_lattice *h, int on);
+/* Solver behind susy_b200_congrad_multi (the host-array drop-in for
+ * congrad_multi.c:26): SUSY_B200_SOLVER_FP64 (default, the reference's
+ * recurrences) or SUSY_B200_SOLVER_MIXED (same FP64 true-residual bound).
+ * Returns the previous setting. */
+int susy_b200_set_solver(susy_b200_lattice *h, int solver);
 /* Mixed-precision solver settings (no reference counterpart): the operator
  * runs in FP32 once |r| < fp32_below |src| (default 3e-4); with the FP32
  * operator the FP64 true residual replaces the iterated one whenever |r|

@@ -291,6 +291,14 @@ int susy_b200_dev_congrad_multi_learned(susy_b200_lattice* h, susy_b200_net* net
                             loose < errormin ? errormin : loose, size_r, iters, refine_iters);
 }
 
+int susy_b200_set_solver(susy_b200_lattice* h, int solver) {
+  if (!h || (solver != SUSY_B200_SOLVER_FP64 && solver != SUSY_B200_SOLVER_MIXED))
+    return SUSY_B200_EINVAL;
+  const int prev = h->host_solver;
+  h->host_solver = solver;
+  return prev;
+}
+
 int susy_b200_use_graphs(susy_b200_lattice* h, int on) {
   if (!h) return SUSY_B200_EINVAL;
   const int prev = h->use_graphs;
@@ -533,7 +541,9 @@ int susy_b200_congrad_multi(susy_b200_lattice* h, const double* src, double* con
   }
   int it = 0;
   double sr = 0.0;
-  r = multishift_fp64(h, s, ps.data(), norder, shift, MaxCG, errormin, &sr, &it);
+  r = h->host_solver == SUSY_B200_SOLVER_MIXED
+          ? multishift_mixed(h, s, ps.data(), norder, shift, MaxCG, errormin, &sr, &it)
+          : multishift_fp64(h, s, ps.data(), norder, shift, MaxCG, errormin, &sr, &it);
   if (r) return r;
   for (int j = 0; j < norder; j++)
     if ((r = susy_b200_tf_download(h, ps[j], 64, psim[j]))) return r;

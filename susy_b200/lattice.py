@@ -156,6 +156,8 @@ def load_library(path: str = LIB_PATH):
     L.susy_b200_plaquette.argtypes = [_vp, _dp, _dp]
     L.susy_b200_mixed_params.restype = C.c_int
     L.susy_b200_mixed_params.argtypes = [_vp, C.c_double, C.c_double]
+    L.susy_b200_set_solver.restype = C.c_int
+    L.susy_b200_set_solver.argtypes = [_vp, C.c_int]
     L.susy_b200_use_graphs.restype = C.c_int
     L.susy_b200_use_graphs.argtypes = [_vp, C.c_int]
     L.susy_b200_cg_blocked.restype = C.c_int
@@ -458,6 +460,10 @@ class Lattice:
         ss, st = C.c_double(), C.c_double()
         self._check(self.lib.susy_b200_plaquette(self.h, C.byref(ss), C.byref(st)))
         return ss.value, st.value
+
+    def set_solver(self, solver: int) -> int:
+        """Solver behind congrad_multi (SOLVER_FP64 or SOLVER_MIXED)."""
+        return self._check(self.lib.susy_b200_set_solver(self.h, int(solver)))
 
     def use_graphs(self, on: int = -1) -> int:
         """CUDA-graph replay (1) or plain launches (0) of the solver's
