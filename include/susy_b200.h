@@ -181,6 +181,7 @@ int susy_b200_set_solver(susy_b200_lattice *h, int solver);
  * fell by reliable_factor (default 1e-2) since the last replacement.
  * 0 < fp32_below <= 1, 0 < reliable_factor < 1, else SUSY_B200_EINVAL. */
 int susy_b200_mixed_params(susy_b200_lattice *h, double fp32_below, double reliable_factor);
+#define SUSY_B200_FOP_NVARIANTS 10   /* entries of ms_per_variant */
 int susy_b200_autotune(susy_b200_lattice *h);
 int susy_b200_fop_variant(susy_b200_lattice *h, int prec, int set_to, float *ms_per_variant);
 int susy_b200_dev_DSq(susy_b200_lattice *h, const void *src, void *dst, int prec);

@@ -98,6 +98,8 @@ static int launch_variant(susy_b200_lattice* h, const void* src, void* dst, int 
 // Project-written autotuner: time one D^dag D with every kernel variant on
 // this lattice and keep the fastest for this precision.  Runs on the first
 // operator call of each precision (before any stream capture).
+static_assert(FOP_NVARIANTS == SUSY_B200_FOP_NVARIANTS, "variant count");
+
 int autotune_fop(susy_b200_lattice* h, int prec) {
   const int pi = prec == 64 ? 0 : 1;
   void* a = scratch_tf(h, 6, prec);

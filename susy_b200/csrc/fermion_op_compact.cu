@@ -413,8 +413,8 @@ SUSY_D void run_pattern_pp(ACC& acc, const FopArgs<R>& a, int s, unsigned bcm, i
 
 // Block order: site-major (SM = true) or component-major; PP: two operand
 // buffers (prefetch) or one.
-template <int N, typename R, int SIGN, bool SM, bool PP>
-__global__ void __launch_bounds__(CT_THREADS)
+template <int N, typename R, int SIGN, bool SM, bool PP, int MINB>
+__global__ void __launch_bounds__(CT_THREADS, MINB)
 fermion_op_pp_kernel(FopArgs<R> a) {
   if (a.skip && *a.skip) return;
   const int comp = SM ? blockIdx.x % NTF : blockIdx.x / a.nsb;
@@ -449,14 +449,14 @@ static int launch_compact(FopArgs<R> a, int sign, cudaStream_t st) {
   return nblk;
 }
 
-template <int N, typename R, bool SM, bool PP>
+template <int N, typename R, bool SM, bool PP, int MINB = 1>
 static int launch_pp(FopArgs<R> a, int sign, cudaStream_t st) {
   a.nsb = (a.g.V + CT_THREADS - 1) / CT_THREADS;
   const int nblk = a.nsb * NTF;
   if (sign > 0)
-    count_launch(), fermion_op_pp_kernel<N, R, 1, SM, PP><<<nblk, CT_THREADS, 0, st>>>(a);
+    count_launch(), fermion_op_pp_kernel<N, R, 1, SM, PP, MINB><<<nblk, CT_THREADS, 0, st>>>(a);
   else
-    count_launch(), fermion_op_pp_kernel<N, R, -1, SM, PP><<<nblk, CT_THREADS, 0, st>>>(a);
+    count_launch(), fermion_op_pp_kernel<N, R, -1, SM, PP, MINB><<<nblk, CT_THREADS, 0, st>>>(a);
   return nblk;
 }
 
@@ -484,11 +484,23 @@ int fermion_op_compact(const FopArgs<R>& a, int N, int sign, int variant, cudaSt
         case 3: return launch_pp<3, R, false, true>(a, sign, st);
         default: return launch_pp<4, R, false, true>(a, sign, st);
       }
-    default:
+    case FOP_SITE_MAJOR:
       switch (N) {
         case 2: return launch_pp<2, R, true, false>(a, sign, st);
         case 3: return launch_pp<3, R, true, false>(a, sign, st);
         default: return launch_pp<4, R, true, false>(a, sign, st);
+      }
+    case FOP_SITE_MAJOR_OCC:
+      switch (N) {
+        case 2: return launch_pp<2, R, true, false, 4>(a, sign, st);
+        case 3: return launch_pp<3, R, true, false, 4>(a, sign, st);
+        default: return launch_pp<4, R, true, false, 4>(a, sign, st);
+      }
+    default:
+      switch (N) {
+        case 2: return launch_pp<2, R, false, false, 8>(a, sign, st);
+        case 3: return launch_pp<3, R, false, false, 8>(a, sign, st);
+        default: return launch_pp<4, R, false, false, 8>(a, sign, st);
       }
   }
 }

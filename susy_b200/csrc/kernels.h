@@ -64,9 +64,17 @@ struct MsBlockVecs {
 // FOP_COMPACT_PF also prefetches the next product's operands.
 // FOP_SITE_MAJOR_PP / FOP_COMP_MAJOR_PP: table-driven with two alternating
 // operand buffers, site-major or component-major block order;
-// FOP_SITE_MAJOR: site-major with one operand buffer (fewest registers).
+// FOP_SITE_MAJOR: site-major with one operand buffer (fewest registers);
+// FOP_SITE_MAJOR_OCC / FOP_COMP_MAJOR_OCC: one buffer with the registers
+// capped for 4 / 8 resident blocks of 128 threads per SM (128 / 64
+// registers per thread): more resident warps to hide the L2 latency the
+// operand gathers wait on, against a little spilling.  Measured at
+// 12^3x24 U(3): the FP64 optimum is the 128-register site-major kernel
+// (0.215 ms vs 0.260 uncapped; 102 registers: 0.256, 64: 0.59), the FP32 one
+// the 64-register component-major kernel (0.117 ms vs 0.135; 48: 0.166).
 enum { FOP_MAT = 0, FOP_MAT_CM = 1, FOP_ROWS = 2, FOP_COMPACT = 3, FOP_COMPACT_PF = 4,
-       FOP_SITE_MAJOR_PP = 5, FOP_COMP_MAJOR_PP = 6, FOP_SITE_MAJOR = 7, FOP_NVARIANTS = 8 };
+       FOP_SITE_MAJOR_PP = 5, FOP_COMP_MAJOR_PP = 6, FOP_SITE_MAJOR = 7,
+       FOP_SITE_MAJOR_OCC = 8, FOP_COMP_MAJOR_OCC = 9, FOP_NVARIANTS = 10 };
 template <typename R>
 int fermion_op(const Geo& g, int N, const void* U, const void* Uinv, const void* pd,
                 const void* src, void* dst, int sign, double G, const void* add, double addc,

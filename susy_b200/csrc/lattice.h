@@ -54,7 +54,7 @@ struct susy_b200_lattice {
   std::vector<void*> gsrc, gr_psim, traj_psim, extra5, refine;
   susy::HostPrn node_prn = {};
   int fop_variant[2] = {-1, -1};  // chosen operator kernel (FP64, FP32); -1 = tune
-  float fop_ms[2][8] = {};        // autotuner timings per variant
+  float fop_ms[2][SUSY_B200_FOP_NVARIANTS] = {};  // autotuner timings per variant
   int err = 0, cuda_err = 0;
 };
 

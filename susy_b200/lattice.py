@@ -48,7 +48,7 @@ SOLVER_FP64 = 0
 SOLVER_MIXED = 1
 HMC = 0
 SMD = 1
-FOP_NVARIANTS = 8
+FOP_NVARIANTS = 10
 
 
 class Meas(C.Structure):
@@ -477,7 +477,7 @@ class Lattice:
 
     def fop_variant(self, prec: int = 64, set_to: int = -1):
         """(current variant, autotuner ms per variant) for one precision."""
-        ms = (C.c_float * 8)()
+        ms = (C.c_float * FOP_NVARIANTS)()
         v = self._check(self.lib.susy_b200_fop_variant(self.h, prec, set_to, ms))
         return v, [ms[i] for i in range(FOP_NVARIANTS)]
 
