@@ -537,6 +537,41 @@ def run_batch_case(args):
                       "cg_iterations": sum(b["iters"] for b in batched)}), flush=True)
 
 
+def run_traj_case(args):
+    """One full RHMC trajectory of the bench lattice with the trajectory
+    parameters of the metric's configuration (12^3x24 U(3), lambda 2,
+    bmass 0.3, G 0.05, degree-15 rational approximation, Nroot 2, 15
+    fermion steps x 3 gauge steps, error_per_site 1e-10, traj_length 1),
+    from the seeded near-identity links (not thermalised).  After one
+    warm-up trajectory, --steps trajectories are timed with CUDA events on
+    the lattice's stream (each trajectory's host work included)."""
+    import torch
+    from susy_b200 import Lattice, RHMC, synth
+    lat = Lattice(DIMS, NCOL, pbc=-1, lam=LAM, bmass=BMASS, G=G)
+    st = torch.cuda.Stream()
+    lat.set_stream(st.cuda_stream)
+    lat.set_links(synth.to_ref(DIMS, synth.links(DIMS, NCOL, LINK_NOISE, LINK_SEED)))
+    out = []
+    for solver in (1, 0):
+        r = RHMC(NORDER, NROOT, nstep=15, nstep_gauge=3, traj_length=1.0, niter=MAXCG,
+                 error_per_site=1e-10, solver=solver)
+        lat.update(r)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        res = [lat.update(r) for _ in range(args.steps)]
+        e1.record(st)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / args.steps
+        out.append({"solver": "mixed" if solver else "fp64", "s_per_traj": ms / 1e3,
+                    "cg_iterations": [t["iters"] for t in res],
+                    "delta_S": [t["delta_S"] for t in res],
+                    "accept": [t["accept"] for t in res]})
+    print(json.dumps({"case": "rhmc_trajectory", "lattice": "12x12x12x24", "ncol": NCOL,
+                      "nstep": 15, "nstep_gauge": 3, "nroot": NROOT, "norder": NORDER,
+                      "runs": out}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -551,6 +586,8 @@ def main():
     ap.add_argument("--variant", type=int, default=-1)
     ap.add_argument("--batch-case", action="store_true",
                     help="independent U(2) lattices of uneven volume, batched vs one by one")
+    ap.add_argument("--traj-case", action="store_true",
+                    help="full RHMC trajectories of the bench lattice, mixed and FP64 solver")
     ap.add_argument("--lattices", type=int, default=48)
     ap.add_argument("--threads", type=int, default=16)
     args = ap.parse_args()
@@ -559,6 +596,9 @@ def main():
         return
     if args.batch_case:
         run_batch_case(args)
+        return
+    if args.traj_case:
+        run_traj_case(args)
         return
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
