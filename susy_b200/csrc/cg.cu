@@ -429,15 +429,16 @@ __global__ void __launch_bounds__(UT) k_msb_update_r(MsState* st, MsBlockVecs v,
   const double b0 = st->beta_i[0];
   const double2* rin = (const double2*)v.ring[(it - 1) % (MS_BLK + 1)];
   double2* rout = (double2*)v.ring[it % (MS_BLK + 1)];
-  const long i = (long)blockIdx.x * UT + threadIdx.x;
+  const MT* mp = (const MT*)(sizeof(MT) == 16 ? v.mp : v.mp32);
   double acc = 0.0;
-  if (i < n) {
+  // grid-stride: few blocks, so the scalar kernel sums few partials
+  for (long i = (long)blockIdx.x * UT + threadIdx.x; i < n; i += (long)gridDim.x * UT) {
     double2 r = rin[i];
-    const MT m = ((const MT*)(sizeof(MT) == 16 ? v.mp : v.mp32))[i];
+    const MT m = mp[i];
     r.x += b0 * m.x;
     r.y += b0 * m.y;
     rout[i] = r;
-    acc = r.x * r.x + r.y * r.y;
+    acc += r.x * r.x + r.y * r.y;
   }
   acc = block_sum<UT>(acc);
   if (threadIdx.x == 0) part[blockIdx.x] = acc;
@@ -596,12 +597,16 @@ __global__ void k_msb_block_reset(MsState* st) {
   }
 }
 
-void msb_update_r(MsState* st, const MsBlockVecs& v, long n, double* part, bool mp32,
-                  cudaStream_t s) {
+// Returns the number of partials written (at most 8 blocks per SM of a
+// 148-SM B200)
+int msb_update_r(MsState* st, const MsBlockVecs& v, long n, double* part, bool mp32,
+                 cudaStream_t s) {
+  const int nb = vec_blocks(n) < 1184 ? vec_blocks(n) : 1184;
   if (mp32)
-    count_launch(), k_msb_update_r<float2><<<vec_blocks(n), UT, 0, s>>>(st, v, n, part);
+    count_launch(), k_msb_update_r<float2><<<nb, UT, 0, s>>>(st, v, n, part);
   else
-    count_launch(), k_msb_update_r<double2><<<vec_blocks(n), UT, 0, s>>>(st, v, n, part);
+    count_launch(), k_msb_update_r<double2><<<nb, UT, 0, s>>>(st, v, n, part);
+  return nb;
 }
 
 // Residual replacement: r(k) <- rt with the matching search-vector

@@ -121,8 +121,8 @@ void ms_update_p0(MsState* st, const MsVecs& v, int prec, long n, cudaStream_t s
 void norm2_partials(const void* x, int prec, long n, double* part, cudaStream_t s);
 int rdot_partials(long n, const void* a, const void* b, double* part, cudaStream_t s);
 void copy_field(long n, const void* a, void* b, cudaStream_t s);
-void msb_update_r(MsState* st, const MsBlockVecs& v, long n, double* part, bool mp32,
-                  cudaStream_t s);
+int msb_update_r(MsState* st, const MsBlockVecs& v, long n, double* part, bool mp32,
+                 cudaStream_t s);
 void msb_replace(MsState* st, const MsBlockVecs& v, long n, const void* rt, double rsq,
                  cudaStream_t s);
 void msb_update_p0(MsState* st, const MsBlockVecs& v, long n, cudaStream_t s);

@@ -228,7 +228,6 @@ static int ms_run_block(susy_b200_lattice* h, const void* src, void* const* psim
   if (errormin_base > 0.0) ms_set_stop(h->ms, errormin_base, s);
 
   const double fm2 = h->prm.fmass > 1e-8 ? h->prm.fmass * h->prm.fmass : 0.0;
-  const int np_vec = vec_blocks(n);
   const int* skip = &h->ms->skip;
   const int chunk = 2 * MS_BLK;
   double* pd = (double*)(pw + 2);  // pinned: the iterated |r|^2
@@ -257,8 +256,8 @@ static int ms_run_block(susy_b200_lattice* h, const void* src, void* const* psim
         np_fop = dev_fop(h, tmp, mp, -1, 64, p0, fm2 + shift[0], part0, skip);
       }
       ms_scalars1(h->ms, part0, np_fop, s);
-      msb_update_r(h->ms, v, n, part1, fp32_op, s);
-      ms_scalars2(h->ms, part1, np_vec, s);
+      const int np_r = msb_update_r(h->ms, v, n, part1, fp32_op, s);
+      ms_scalars2(h->ms, part1, np_r, s);
       msb_update_p0(h->ms, v, n, s);
       if ((k + 1) % MS_BLK == 0) msb_block(h->ms, v, n, s);
     }
