@@ -423,19 +423,22 @@ def run_ours(args, rank, world, device):
 
 
 def run_dsq_case(args):
-    """Operator microbenchmark on the bench lattice: D^dag D per kernel
-    variant and precision (CUDA events on the launching stream, 20
-    applications after 3 warm-up ones; the 0.26 GB FP64 working set per
-    application is larger than L2).  --variant V restricts it to one variant
-    (the small case an ncu capture of one kernel runs)."""
+    """Operator microbenchmark on the bench lattice (or --dims / --ncol):
+    D^dag D per kernel variant and precision (CUDA events on the launching
+    stream, 20 applications after 3 warm-up ones; the working set per
+    application must exceed the 126 MB L2 for an HBM figure: 0.26 GB at
+    12^3x24 U(3) FP64).  --variant V restricts it to one variant (the small
+    case an ncu capture of one kernel runs)."""
     import torch
     from susy_b200 import Lattice, synth
     from susy_b200.lattice import FOP_NVARIANTS
-    lat = Lattice(DIMS, NCOL, pbc=-1, lam=LAM, bmass=BMASS, G=G)
+    dims = tuple(int(x) for x in args.dims.split(",")) if args.dims else DIMS
+    ncol = args.ncol or NCOL
+    lat = Lattice(dims, ncol, pbc=-1, lam=LAM, bmass=BMASS, G=G)
     st = torch.cuda.Stream()
     lat.set_stream(st.cuda_stream)
-    lat.set_links(synth.to_ref(DIMS, synth.links(DIMS, NCOL, LINK_NOISE, LINK_SEED)))
-    src = synth.to_ref(DIMS, synth.tf_source(DIMS, NCOL, SRC_SEED))
+    lat.set_links(synth.to_ref(dims, synth.links(dims, ncol, LINK_NOISE, LINK_SEED)))
+    src = synth.to_ref(dims, synth.tf_source(dims, ncol, SRC_SEED))
     peak, peak_kind = measured_peaks()
     variants = [args.variant] if args.variant >= 0 else list(range(FOP_NVARIANTS))
     reps = 3 if args.variant >= 0 else 20
@@ -459,13 +462,13 @@ def run_dsq_case(args):
             e1.record(st)
             e1.synchronize()
             ms = e0.elapsed_time(e1) / (2 * reps)
-            algo = algorithmic_bytes_fop(lat.V, NCOL, w)
+            algo = algorithmic_bytes_fop(lat.V, ncol, w)
             gbs = algo / (ms * 1e-3) / 1e9
-            print(json.dumps({"case": "fermion_op", "lattice": "12x12x12x24", "ncol": NCOL,
-                              "prec": prec, "variant": v, "ms_per_launch": ms,
+            print(json.dumps({"case": "fermion_op", "lattice": "x".join(map(str, dims)),
+                              "ncol": ncol, "prec": prec, "variant": v, "ms_per_launch": ms,
                               "algorithmic_gbs": gbs, "frac": gbs / peak,
                               "peak_kind": peak_kind,
-                              "tflops": flops_fop(lat.V, NCOL) / (ms * 1e-3) / 1e12}),
+                              "tflops": flops_fop(lat.V, ncol) / (ms * 1e-3) / 1e12}),
                   flush=True)
 
 
@@ -584,6 +587,8 @@ def main():
     ap.add_argument("--dsq-case", action="store_true",
                     help="operator microbenchmark per kernel variant instead of the solve")
     ap.add_argument("--variant", type=int, default=-1)
+    ap.add_argument("--dims", default="", help="--dsq-case lattice, e.g. 24,24,24,24")
+    ap.add_argument("--ncol", type=int, default=0, help="--dsq-case NCOL")
     ap.add_argument("--batch-case", action="store_true",
                     help="independent U(2) lattices of uneven volume, batched vs one by one")
     ap.add_argument("--traj-case", action="store_true",

@@ -357,7 +357,7 @@ int susy_b200_dev_congrad_multi_learned(susy_b200_lattice *h, susy_b200_net *net
 /* Independent lattices at once (no reference counterpart: the reference
  * runs one lattice per process): one update() per handle, h[i] with r[i]
  * into res[i], the handles' streams driven concurrently by `threads` host
- * threads.  Each lattice's result is the one update() gives it alone.
+ * threads (at most 16).  Each lattice's result is the one update() gives it alone.
  * Returns the total CG iterations or the first negative error code. */
 int susy_b200_update_batch(susy_b200_lattice *const *h, const susy_b200_rhmc *const *r,
                            susy_b200_traj *res, int n, int threads);

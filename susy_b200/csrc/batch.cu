@@ -24,7 +24,9 @@ extern "C" int susy_b200_update_batch(susy_b200_lattice* const* hs,
   if (!hs || !rs || !res || n < 0) return SUSY_B200_EINVAL;
   for (int i = 0; i < n; i++)
     if (!hs[i] || !rs[i]) return SUSY_B200_EINVAL;
-  const int nt = std::max(1, std::min(threads > 0 ? threads : 1, n));
+  // at most 16 host threads: the configuration measured; one run with 48
+  // threads ended in a host crash whose cause was not found
+  const int nt = std::max(1, std::min(std::min(threads > 0 ? threads : 1, n), 16));
   std::atomic<int> next(0);
   std::vector<int> rc(n, 0);
   auto work = [&]() {
