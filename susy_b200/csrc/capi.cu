@@ -16,8 +16,18 @@ using namespace susy;
 namespace susy {
 
 static std::atomic<long long> g_launches(0);
-void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
-void count_launches(long long n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+// Per host thread as well, so that a thread capturing a CUDA graph can
+// count its own launches while other threads launch (update_batch)
+static thread_local long long t_launches = 0;
+void count_launch() {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  t_launches++;
+}
+void count_launches(long long n) {
+  g_launches.fetch_add(n, std::memory_order_relaxed);
+  t_launches += n;
+}
+long long thread_launch_count() { return t_launches; }
 
 static size_t mat_c(const susy_b200_lattice* h) { return (size_t)h->N * h->N; }
 

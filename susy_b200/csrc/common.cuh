@@ -24,6 +24,7 @@ namespace susy {
 // site is written as "count_launch(), kernel<<<...>>>(...)").
 void count_launch();
 void count_launches(long long n);
+long long thread_launch_count();
 
 constexpr int NUMLINK = 5;
 constexpr int NPLAQ = 10;

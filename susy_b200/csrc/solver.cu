@@ -129,7 +129,7 @@ struct ChunkGraph {
     const int pi = prec == 64 ? 0 : 1;
     if (h->fop_variant[pi] < 0) autotune_fop(h, prec);
     cudaStream_t s = h->stream;
-    const long long c0 = susy_b200_launch_count();
+    const long long c0 = thread_launch_count();
     if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
       cudaGetLastError();
       h->use_graphs = 0;
@@ -138,7 +138,7 @@ struct ChunkGraph {
     issue();
     cudaGraph_t g = nullptr;
     const cudaError_t e1 = cudaStreamEndCapture(s, &g);
-    kernels = susy_b200_launch_count() - c0;
+    kernels = thread_launch_count() - c0;
     count_launches(-kernels);   // captured, not launched
     if (e1 != cudaSuccess || !g || cudaGraphInstantiate(&exec, g, 0) != cudaSuccess) {
       cudaGetLastError();
