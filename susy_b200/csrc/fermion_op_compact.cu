@@ -222,6 +222,28 @@ SUSY_D void run_pattern(Mat<N, R>& acc, const FopArgs<R>& a, int s, unsigned bcm
   }
 }
 
+// Tr(A op(B)) for A = component ka of fa at site sa and B = component kb of
+// fb at site sb (op(B) = B^dag when ADJB), one element pair at a time: the
+// determinant terms run while the accumulator is live, and holding whole
+// matrices here made the register-capped kernels spill
+template <int N, typename R, bool ADJB>
+SUSY_D Cx<R> trace_ld(const typename CT<R>::T* fa, int ka, int sa, const typename CT<R>::T* fb,
+                      int kb, int sb, int S) {
+  const typename CT<R>::T* pa = fa + (size_t)(ka * N * N) * S + sa;
+  const typename CT<R>::T* pb = fb + (size_t)(kb * N * N) * S + sb;
+  Cx<R> t(0, 0);
+#pragma unroll
+  for (int i = 0; i < N; i++)
+#pragma unroll
+    for (int k = 0; k < N; k++) {
+      const Cx<R> x = ldc<R>(pa + (size_t)(i * N + k) * S);
+      const Cx<R> y = ADJB ? conj(ldc<R>(pb + (size_t)(i * N + k) * S))
+                           : ldc<R>(pb + (size_t)(k * N + i) * S);
+      t = t + x * y;
+    }
+  return t;
+}
+
 // detStoL for output link B (utilities.c:551-628)
 template <int N, typename R, int SIGN>
 SUSY_D void det_stol_rt(Mat<N, R>& acc, const FopArgs<R>& a, const Site& c, int B) {
@@ -238,8 +260,12 @@ SUSY_D void det_stol_rt(Mat<N, R>& acc, const FopArgs<R>& a, const Site& c, int 
     const Cx<R> trm = ldtr<N, R, ADJ>(a.src, 0, mE, S);
     tsum = tsum + bcf<R>(g, c, -et(e)) * (trm * ldc<R>(a.pd + (size_t)(B * 5 + e) * S + mE));
   }
-  Mat<N, R> ui = ldm<N, R>(a.Uinv, B, s, S);
-  axpy(acc, ((R)(-0.5) * a.G) * tsum, ui);
+  const Cx<R> f = ((R)(-0.5) * a.G) * tsum;
+  const typename CT<R>::T* pu = a.Uinv + (size_t)(B * N * N) * S + s;
+#pragma unroll
+  for (int i = 0; i < N; i++)
+#pragma unroll
+    for (int j = 0; j < N; j++) acc.e[i][j] = acc.e[i][j] + f * ldc<R>(pu + (size_t)(i * N + j) * S);
 }
 
 // detLtoS for the site output (utilities.c:688-756)
@@ -250,8 +276,7 @@ SUSY_D void det_ltos_rt(Mat<N, R>& acc, const FopArgs<R>& a, const Site& c) {
   const int S = g.S, s = c.s;
   Cx<R> T0[NUMLINK];
 #pragma unroll
-  for (int e = 0; e < NUMLINK; e++)
-    T0[e] = trace_nn(ldm<N, R>(a.Uinv, e, s, S), ldm<N, R, ADJ>(a.src, 1 + e, s, S));
+  for (int e = 0; e < NUMLINK; e++) T0[e] = trace_ld<N, R, ADJ>(a.Uinv, e, s, a.src, 1 + e, s, S);
   Cx<R> tsum(0, 0);
 #pragma unroll 1
   for (int b = 0; b < NUMLINK; b++) {
@@ -264,7 +289,7 @@ SUSY_D void det_ltos_rt(Mat<N, R>& acc, const FopArgs<R>& a, const Site& c) {
 #pragma unroll 1
     for (int e = 0; e < NUMLINK; e++) {
       if (e == b) continue;
-      const Cx<R> Tp = trace_nn(ldm<N, R>(a.Uinv, e, pb, S), ldm<N, R, ADJ>(a.src, 1 + e, pb, S));
+      const Cx<R> Tp = trace_ld<N, R, ADJ>(a.Uinv, e, pb, a.src, 1 + e, pb, S);
       tsum = tsum + ldc<R>(a.pd + (size_t)(e * 5 + b) * S + s) * (T0b + bcb * Tp);
     }
   }
