@@ -16,7 +16,14 @@ Writes
                            the run parameters of testsuite/in.U{2,3}.hmc;
   config_U2_4444.npz, config_U3_4444.npz
                            the starting links of those runs (testsuite/
-                           config.U{2,3}.4444, read with susy_b200.io_lat).
+                           config.U{2,3}.4444, read with susy_b200.io_lat);
+  config0_U2.json          the reference run through the harness on the
+                           4^4 U(2) configuration the benchmark's first
+                           config names (identity + 0.05 noise links from
+                           synth.links seed 0, lambda 1, bmass 0.2, G 0.05,
+                           Nroot 1, Norder 15, 10 x 2 steps, error_per_site
+                           1e-10): two trajectories' action lines, delta S,
+                           accept, IT_PER_TRAJ and force monitors.
 """
 import json
 import os
@@ -127,7 +134,10 @@ def _fermion_force_with_amps(ref, eps, src, sols, amp):
 
 
 def parse_hmc_ref(path):
-    txt = open(path).read()
+    return parse_hmc_text(open(path).read())
+
+
+def parse_hmc_text(txt):
     trajs = []
     acts = re.findall(r"action: gauge (\S+) bmass (\S+) det (\S+) fermion0 (\S+) mom (\S+) sum (\S+)",
                       txt)
@@ -141,7 +151,8 @@ def parse_hmc_ref(path):
                           start_S=float(acc[k][2]), end_S=float(acc[k][3]),
                           it_per_traj=int(its[k]),
                           monitor=[float(x) for x in mon[k]]))
-    start = re.search(r"START (\S+) (\S+) (\S+) (\S+)", txt).groups()
+    start = re.search(r"START (\S+) (\S+) (\S+) (\S+)", txt)
+    start = start.groups() if start else ()
     # measurement lines (control.c:52-68 at start, :85-138 per trajectory)
     nums = lambda line: [float(x) for x in line.split()[1:]]
     lines = txt.splitlines()
@@ -172,6 +183,28 @@ def trajs_started(lines, line):
     return any(l.startswith("IT_PER_TRAJ") for l in lines[:i])
 
 
+CONFIG0 = dict(dims=(4, 4, 4, 4), pbc=-1, iseed=41, Nroot=1, Norder=15, traj_length=1.0,
+               nstep=10, nstep_gauge=2, lam=1.0, kappa_u1=0.0, bmass=0.2, fmass=0.0, G=0.05,
+               max_cg=5000, error_per_site=1e-10)
+CONFIG0_LINKS = dict(noise=0.05, seed=0)
+
+
+def config0_job(ntraj=2):
+    from oracle.ref_ctypes import RefLattice
+    from susy_b200 import synth
+    ref = RefLattice(2, **CONFIG0)
+    U = synth.links(CONFIG0["dims"], 2, CONFIG0_LINKS["noise"], CONFIG0_LINKS["seed"])
+    ref.set_links(synth.to_ref(CONFIG0["dims"], U))
+    ref.set_mom(np.zeros_like(synth.to_ref(CONFIG0["dims"], U)))
+    ref.compute_all()
+    out = []
+    for _ in range(ntraj):
+        start = len(ref.log())
+        ref.update()
+        out.append(parse_hmc_text(ref.log()[start:])["trajectories"][0])
+    return out
+
+
 def parse_input(path):
     kv = {}
     for line in open(path):
@@ -198,6 +231,12 @@ def main():
         np.savez(os.path.join(HERE, "config_U%d_4444.npz" % N), dims=np.array(dims),
                  links=links.astype(np.complex64), sum29=info["sum29"], sum31=info["sum31"])
         print("hmc_U%d.json: %d trajectories" % (N, len(d["trajectories"])))
+    c0 = run_in_fresh_process(config0_job)
+    with open(os.path.join(HERE, "config0_U2.json"), "w") as f:
+        json.dump({"params": {k: list(v) if isinstance(v, tuple) else v
+                              for k, v in CONFIG0.items()},
+                   "links": CONFIG0_LINKS, "trajectories": c0}, f, indent=1)
+    print("config0_U2.json: %d trajectories" % len(c0))
 
 
 if __name__ == "__main__":

@@ -97,3 +97,49 @@ def test_graph_replay_matches_plain_launches(mixed):
     assert out[0][0] == out[1][0] and out[0][1] == out[1][1]
     for a, b in zip(out[0][2], out[1][2]):
         assert np.array_equal(a, b)
+
+
+def test_config1_operator_precisions_and_solvers():
+    """The operator and solver microbenchmark configuration (8^4 U(2),
+    links identity + 0.2 noise, lambda 1, bmass 0.2, G 0.05): D^dag D in
+    FP64 and FP32 against the FP64 oracle on complex-Gaussian sources, and
+    the 15-shift solve (shifts 1e-5 ... 1e3, FP64 true residual 1e-10 per
+    site) with the FP64 and the mixed solver: same bound for every shift,
+    solutions agreeing to 1e-8."""
+    dims, N = (8, 8, 8, 8), 2
+    U = synth.links(dims, N, 0.2, 1)
+    lat = Lattice(dims, N, pbc=-1, lam=1.0, bmass=0.2, G=0.05)
+    lat.set_links(synth.to_ref(dims, U))
+    geo = O.Geometry(dims, -1)
+    prm = O.Params(lam=1.0, bmass=0.2, G=0.05, N=N)
+    der = O.compute_derived(geo, prm, U)
+    for k in range(2):
+        src = synth.tf_source(dims, N, 50 + k)
+        want = O.DSq(geo, prm, U, der, src)
+        a, b = lat.tf(64), lat.tf(64)
+        a.upload(synth.to_ref(dims, src))
+        lat.dev_DSq(a, b)
+        got = synth.from_ref(dims, b.download(), 16, N)
+        assert np.abs(got - want).max() <= 1e-13 * np.abs(want).max()
+        a32, b32 = lat.tf(32), lat.tf(32)
+        lat.dev_convert(a, a32)
+        lat.dev_DSq(a32, b32)
+        lat.dev_convert(b32, b)
+        got = synth.from_ref(dims, b.download(), 16, N)
+        assert np.abs(got - want).max() <= 2e-6 * np.abs(want).max()
+    shifts = synth.geometric_shifts(15, 1e-5, 1e3)
+    src = lat.tf(64)
+    src.upload(synth.to_ref(dims, synth.tf_source(dims, N, 60)))
+    b2 = float(np.dot(src.download(), src.download()))
+    sols = {}
+    for mixed in (False, True):
+        psim = [lat.tf(64) for _ in shifts]
+        lat.dev_congrad_multi(src, psim, shifts, 20000, 1e-20, mixed=mixed)
+        sols[mixed] = [p.download() for p in psim]
+        t = lat.tf(64)
+        for j, s in enumerate(shifts):
+            lat.dev_DSq(psim[j], t)
+            r = src.download() - t.download() - s * sols[mixed][j]
+            assert float(np.dot(r, r)) <= 1.5e-20 * b2
+    for x, y in zip(sols[False], sols[True]):
+        assert np.abs(x - y).max() <= 1e-8 * np.abs(x).max()

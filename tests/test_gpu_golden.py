@@ -145,3 +145,33 @@ def test_smd_with_full_refresh_is_the_hmc_regression_run():
         assert g["accept"] == t["accept"]
         assert abs(g["start"] - t["start_S"]) < 1e-6
         assert abs(g["end"] - t["end_S"]) < 1e-6
+
+
+def test_config0_trajectories_match_the_reference():
+    """The 4^4 U(2) configuration of the benchmark's first config (identity
+    + 0.05 noise links, lambda 1, bmass 0.2, G 0.05, B = kappa_u1 = 0,
+    Nroot 1, 10 x 2 steps, error_per_site 1e-10, seed 41) run by the
+    reference itself through the harness (tests/golden/config0_U2.json):
+    two trajectories on the GPU reproduce its action pieces, delta S,
+    accept and force monitors."""
+    gold = json.load(open(os.path.join(GOLD, "config0_U2.json")))
+    p = gold["params"]
+    dims = tuple(p["dims"])
+    lat = Lattice(dims, 2, pbc=p["pbc"], lam=p["lam"], bmass=p["bmass"], fmass=p["fmass"],
+                  kappa_u1=p["kappa_u1"], G=p["G"], iseed=p["iseed"])
+    U = synth.links(dims, 2, gold["links"]["noise"], gold["links"]["seed"])
+    lat.set_links(synth.to_ref(dims, U))
+    r = RHMC(p["Norder"], p["Nroot"], nstep=p["nstep"], nstep_gauge=p["nstep_gauge"],
+             traj_length=p["traj_length"], niter=p["max_cg"],
+             error_per_site=p["error_per_site"])
+    for t in gold["trajectories"]:
+        g = lat.update(r)
+        for a, b in zip(g["start_parts"], t["start_action"][:5]):
+            assert abs(a - b) <= 5e-8 * max(abs(b), 1e-3)
+        for a, b in zip(g["end_parts"], t["end_action"][:5]):
+            assert abs(a - b) <= 5e-8 * max(abs(b), 1e-3)
+        assert g["accept"] == t["accept"]
+        assert abs(g["delta_S"] - t["delta_S"]) <= 1e-3 * max(abs(t["delta_S"]), 1e-3)
+        assert abs(g["iters"] - t["it_per_traj"]) <= 12
+        assert g["gnorm"] == pytest.approx(t["monitor"][0], rel=2e-3)
+        assert g["fnorm"][0] == pytest.approx(t["monitor"][2], rel=2e-3)
