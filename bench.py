@@ -44,6 +44,7 @@ DIMS = (12, 12, 12, 24)
 NCOL = 3
 LAM, BMASS, G = 2.0, 0.3, 0.05
 LINK_NOISE, LINK_SEED, SRC_SEED = 0.1, 11, 12
+TRAJ_SEED = 13
 NORDER, NROOT = 15, 2
 ERRORMIN = 1e-20          # error_per_site 1e-10 squared (setup.c:356-359)
 MAXCG = 20000
@@ -541,24 +542,36 @@ def run_batch_case(args):
 
 
 def run_traj_case(args):
-    """One full RHMC trajectory of the bench lattice with the trajectory
+    """Full RHMC trajectories of the bench lattice with the trajectory
     parameters of the metric's configuration (12^3x24 U(3), lambda 2,
     bmass 0.3, G 0.05, degree-15 rational approximation, Nroot 2, 15
     fermion steps x 3 gauge steps, error_per_site 1e-10, traj_length 1),
-    from the seeded near-identity links (not thermalised).  After one
-    warm-up trajectory, --steps trajectories are timed with CUDA events on
-    the lattice's stream (each trajectory's host work included)."""
+    from the seeded near-identity links (not thermalised).  One warm-up
+    trajectory (mixed solver) moves the links off the start; then each
+    solver runs --steps trajectories from those same links and the same
+    random-number state (so every solver integrates the same trajectory and
+    only the solves differ), timed with CUDA events on the lattice's stream
+    (each trajectory's host work included).  Solvers: mixed (FP32
+    per-shift corrections), mixed with FP64 corrections, FP64."""
     import torch
     from susy_b200 import Lattice, RHMC, synth
     lat = Lattice(DIMS, NCOL, pbc=-1, lam=LAM, bmass=BMASS, G=G)
     st = torch.cuda.Stream()
     lat.set_stream(st.cuda_stream)
     lat.set_links(synth.to_ref(DIMS, synth.links(DIMS, NCOL, LINK_NOISE, LINK_SEED)))
+    mk = lambda solver: RHMC(NORDER, NROOT, nstep=15, nstep_gauge=3, traj_length=1.0,
+                             niter=MAXCG, error_per_site=1e-10, solver=solver)
+    lat.update(mk(1))
+    start = lat.get_links()
     out = []
-    for solver in (1, 0):
-        r = RHMC(NORDER, NROOT, nstep=15, nstep_gauge=3, traj_length=1.0, niter=MAXCG,
-                 error_per_site=1e-10, solver=solver)
-        lat.update(r)
+    for name, solver, c32 in (("mixed", 1, True), ("mixed_fp64_corrections", 1, False),
+                              ("fp64", 0, True)):
+        if args.traj_solvers and name not in args.traj_solvers.split(","):
+            continue
+        lat.set_links(start)
+        lat.seed(TRAJ_SEED)
+        lat.mixed_correction(c32)
+        r = mk(solver)
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(st)
@@ -566,10 +579,12 @@ def run_traj_case(args):
         e1.record(st)
         e1.synchronize()
         ms = e0.elapsed_time(e1) / args.steps
-        out.append({"solver": "mixed" if solver else "fp64", "s_per_traj": ms / 1e3,
+        out.append({"solver": name, "s_per_traj": ms / 1e3,
                     "cg_iterations": [t["iters"] for t in res],
                     "delta_S": [t["delta_S"] for t in res],
                     "accept": [t["accept"] for t in res]})
+        print(json.dumps(out[-1]), flush=True)
+    lat.mixed_correction(True)
     print(json.dumps({"case": "rhmc_trajectory", "lattice": "12x12x12x24", "ncol": NCOL,
                       "nstep": 15, "nstep_gauge": 3, "nroot": NROOT, "norder": NORDER,
                       "runs": out}), flush=True)
@@ -591,6 +606,8 @@ def main():
     ap.add_argument("--ncol", type=int, default=0, help="--dsq-case NCOL")
     ap.add_argument("--batch-case", action="store_true",
                     help="independent U(2) lattices of uneven volume, batched vs one by one")
+    ap.add_argument("--traj-solvers", default="",
+                    help="with --traj-case: comma list of mixed, mixed_fp64_corrections, fp64")
     ap.add_argument("--traj-case", action="store_true",
                     help="full RHMC trajectories of the bench lattice, mixed and FP64 solver")
     ap.add_argument("--lattices", type=int, default=48)

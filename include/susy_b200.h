@@ -181,6 +181,12 @@ int susy_b200_set_solver(susy_b200_lattice *h, int solver);
  * fell by reliable_factor (default 1e-2) since the last replacement.
  * 0 < fp32_below <= 1, 0 < reliable_factor < 1, else SUSY_B200_EINVAL. */
 int susy_b200_mixed_params(susy_b200_lattice *h, double fp32_below, double reliable_factor);
+/* Mixed solver, after the multi-shift pass: a shift whose FP64 true
+ * residual is above the bound gets correction solves (D^dag D + sigma) e = r,
+ * x += e, with the FP32 operator and recurrences (fp32 = 1, the default;
+ * the FP64 true residual is checked after every pass) or in FP64 (fp32 = 0).
+ * No counterpart in the reference.  fp32 not 0 or 1: SUSY_B200_EINVAL. */
+int susy_b200_mixed_correction(susy_b200_lattice *h, int fp32);
 #define SUSY_B200_FOP_NVARIANTS 10   /* entries of ms_per_variant */
 int susy_b200_autotune(susy_b200_lattice *h);
 int susy_b200_fop_variant(susy_b200_lattice *h, int prec, int set_to, float *ms_per_variant);

@@ -291,6 +291,12 @@ int susy_b200_mixed_params(susy_b200_lattice* h, double fp32_below, double relia
   return SUSY_B200_OK;
 }
 
+int susy_b200_mixed_correction(susy_b200_lattice* h, int fp32) {
+  if (!h || (fp32 != 0 && fp32 != 1)) return SUSY_B200_EINVAL;
+  h->mix_correct32 = fp32;
+  return SUSY_B200_OK;
+}
+
 int susy_b200_dev_congrad_multi_learned(susy_b200_lattice* h, susy_b200_net* net,
                                         const void* src, void* const* psim, int norder,
                                         const double* shift, int MaxCG, double errormin,

@@ -6,8 +6,9 @@
 //                   FP64 reliable updates of the base residual;
 //                   (2) per shift, the FP64 true residual
 //                   r = b - (D^dag D + sigma) x; a shift with
-//                   |r|^2 > errormin |b|^2 gets an FP64 CG on
-//                   (D^dag D + sigma) e = r and x += e.
+//                   |r|^2 > errormin |b|^2 gets CG passes on
+//                   (D^dag D + sigma) e = r, x += e, with the FP32
+//                   operator (FP64 once a pass gains under 10x).
 //                   Every shift ends at or below the FP64 true residual
 //                   bound errormin |b|^2.
 #include <algorithm>
@@ -376,26 +377,41 @@ int multishift_mixed(susy_b200_lattice* h, const void* src, void* const* psim, i
   int total = it1;
   // (2) every shift's FP64 true residual; a shift above the bound (the FP32
   // products leave the shifted systems an error of order FP32 rounding
-  // times the residual at the switch) gets an FP64 correction solve
+  // times the residual at the switch) gets correction solves
+  // (D^dag D + sigma) e = r, x += e.  The correction only needs the leading
+  // digits of e, so it runs with the FP32 operator and FP32 recurrences
+  // (FP64 e), each pass asked for at most 1e-4 in |r| and the FP64 true
+  // residual deciding after it (iterative refinement); a pass that gains
+  // less than 10x in |r|^2 switches the shift's remaining passes to FP64.
   double* part = partials(h, 2);
   void* r64 = refine_field(h, 0, 64);
+  void* r32 = refine_field(h, 0, 32);
   void* e64 = refine_field(h, 1, 64);
-  if (!part || !r64 || !e64) return set_err(h, SUSY_B200_ENOMEM);
+  if (!part || !r64 || !r32 || !e64) return set_err(h, SUSY_B200_ENOMEM);
   norm2_partials(src, 64, n, part, h->stream);
   const double bnorm = host_sum(h, part, vec_blocks(n), 0);
   const double target = errormin * bnorm;
   double worst = 0.0;
   for (int j = 0; j < norder; j++) {
-    double rr = true_residual(h, src, psim[j], shift[j], r64, nullptr);
-    for (int outer = 0; outer < 4 && rr > target && total < MaxCG; outer++) {
+    double rr = true_residual(h, src, psim[j], shift[j], r64, r32);
+    bool fp32 = h->mix_correct32 != 0;
+    for (int outer = 0; outer < 8 && rr > target && total < MaxCG; outer++) {
       void* e[1] = {e64};
       int it2 = 0;
       double s2 = 0.0;
-      rc = ms_run(h, r64, e, 1, &shift[j], MaxCG - total, 0.25 * target / rr, 64, 64, &s2, &it2);
+      if (fp32)
+        rc = ms_run(h, r32, e, 1, &shift[j], MaxCG - total, std::max(0.25 * target / rr, 1e-8),
+                    32, 64, &s2, &it2);
+      else
+        rc = ms_run(h, r64, e, 1, &shift[j], MaxCG - total, 0.25 * target / rr, 64, 64, &s2,
+                    &it2);
       if (rc) return rc;
       total += it2;
       axpy_field(n, 1.0, e64, psim[j], h->stream);
-      rr = true_residual(h, src, psim[j], shift[j], r64, nullptr);
+      const double before = rr;
+      rr = true_residual(h, src, psim[j], shift[j], r64, r32);
+      if (!(rr == rr)) return set_err(h, SUSY_B200_ENAN);
+      if (fp32 && !(rr < 0.1 * before)) fp32 = false;
     }
     worst = std::max(worst, rr);
   }

@@ -156,6 +156,8 @@ def load_library(path: str = LIB_PATH):
     L.susy_b200_plaquette.argtypes = [_vp, _dp, _dp]
     L.susy_b200_mixed_params.restype = C.c_int
     L.susy_b200_mixed_params.argtypes = [_vp, C.c_double, C.c_double]
+    L.susy_b200_mixed_correction.restype = C.c_int
+    L.susy_b200_mixed_correction.argtypes = [_vp, C.c_int]
     L.susy_b200_set_solver.restype = C.c_int
     L.susy_b200_set_solver.argtypes = [_vp, C.c_int]
     L.susy_b200_use_graphs.restype = C.c_int
@@ -432,6 +434,11 @@ class Lattice:
         residual replacement whenever |r| fell by reliable_factor."""
         self._check(self.lib.susy_b200_mixed_params(self.h, float(fp32_below),
                                                     float(reliable_factor)))
+
+    def mixed_correction(self, fp32: bool = True):
+        """Mixed solver: per-shift correction solves with the FP32 operator
+        (iterative refinement against the FP64 true residual) or in FP64."""
+        self._check(self.lib.susy_b200_mixed_correction(self.h, 1 if fp32 else 0))
 
     def measure(self) -> dict:
         """Measurements of control.c:85-138 on the current links, keyed as

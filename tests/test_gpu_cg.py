@@ -143,3 +143,35 @@ def test_config1_operator_precisions_and_solvers():
             assert float(np.dot(r, r)) <= 1.5e-20 * b2
     for x, y in zip(sols[False], sols[True]):
         assert np.abs(x - y).max() <= 1e-8 * np.abs(x).max()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("fp32", [True, False])
+def test_mixed_corrections_meet_bound(fp32):
+    """The mixed solver switched to the FP32 operator early (|r| < 1e-2
+    |src|), so that most shifts need per-shift correction solves: with the
+    FP32 corrections (iterative refinement against the FP64 true residual)
+    and with FP64 ones, every shift ends at the FP64 true-residual bound and
+    agrees with the FP64 solver's solution."""
+    dims, N = (8, 8, 8, 8), 2
+    lat = Lattice(dims, N, pbc=-1, lam=1.0, bmass=0.2, G=0.05)
+    lat.set_links(synth.to_ref(dims, synth.links(dims, N, 0.2, 1)))
+    shifts = synth.geometric_shifts(15, 1e-5, 1e3)
+    src = lat.tf(64)
+    src.upload(synth.to_ref(dims, synth.tf_source(dims, N, 61)))
+    b2 = float(np.dot(src.download(), src.download()))
+    ref = [lat.tf(64) for _ in shifts]
+    lat.dev_congrad_multi(src, ref, shifts, 20000, 1e-20, mixed=False)
+    lat.mixed_params(1e-2, 1e-2)
+    lat.mixed_correction(fp32)
+    psim = [lat.tf(64) for _ in shifts]
+    lat.dev_congrad_multi(src, psim, shifts, 20000, 1e-20, mixed=True)
+    t = lat.tf(64)
+    for j, s in enumerate(shifts):
+        lat.dev_DSq(psim[j], t)
+        x = psim[j].download()
+        r = src.download() - t.download() - s * x
+        assert float(np.dot(r, r)) <= 1.5e-20 * b2
+        y = ref[j].download()
+        assert np.abs(x - y).max() <= 1e-8 * np.abs(y).max()
+    assert lat.lib.susy_b200_mixed_correction(lat.h, 2) < 0
