@@ -146,55 +146,12 @@ SUSY_D void mac(Mat<N, R>& acc, R s, const Mat<N, R>& A, const Mat<N, R>& B) {
     }
 }
 
-// x with its sign bit XORed by bit 31 of m (an integer operation: no
-// floating-point pipe cycle, exact)
-SUSY_D double flip_sign(double x, unsigned m) {
-  return __hiloint2double(__double2hiint(x) ^ (int)m, __double2loint(x));
-}
-SUSY_D float flip_sign(float x, unsigned m) { return __uint_as_float(__float_as_uint(x) ^ m); }
-
-// acc += (-1)^neg A B with m = neg << 31: the sign goes into the right
-// factor's sign bits instead of 2 N^2 multiplies
-template <int N, typename R>
-SUSY_D void mac_sign(Mat<N, R>& acc, unsigned m, const Mat<N, R>& A, const Mat<N, R>& B) {
-  Cx<R> bs[N][N];
-#pragma unroll
-  for (int k = 0; k < N; k++)
-#pragma unroll
-    for (int j = 0; j < N; j++)
-      bs[k][j] = Cx<R>(flip_sign(B.e[k][j].re, m), flip_sign(B.e[k][j].im, m));
-#pragma unroll
-  for (int i = 0; i < N; i++)
-#pragma unroll
-    for (int k = 0; k < N; k++) {
-      const Cx<R> a = A.e[i][k];
-#pragma unroll
-      for (int j = 0; j < N; j++) {
-        R re = acc.e[i][j].re, im = acc.e[i][j].im;
-        re = fma(a.re, bs[k][j].re, re);
-        re = fma(-a.im, bs[k][j].im, re);
-        im = fma(a.re, bs[k][j].im, im);
-        im = fma(a.im, bs[k][j].re, im);
-        acc.e[i][j] = Cx<R>(re, im);
-      }
-    }
-}
-
 // Matrix accumulator of the table-driven operator kernels
 template <int N, typename R>
 struct AccMat {
   Mat<N, R> m;
   SUSY_D void zero() { m.zero(); }
   SUSY_D void add(R s, const Mat<N, R>& A, const Mat<N, R>& B) { mac<0>(m, s, A, B); }
-  SUSY_D void add_sign(unsigned sm, const Mat<N, R>& A, const Mat<N, R>& B) {
-    mac_sign(m, sm, A, B);
-  }
-  SUSY_D void scale(R s) {
-#pragma unroll
-    for (int i = 0; i < N; i++)
-#pragma unroll
-      for (int j = 0; j < N; j++) m.e[i][j] = Cx<R>(s * m.e[i][j].re, s * m.e[i][j].im);
-  }
   SUSY_D Mat<N, R> get() const { return m; }
 };
 

@@ -13,7 +13,6 @@
 // SM's instruction cache (the fully unrolled kernels stall on instruction
 // fetch) and only one or two products' operands are live.  The determinant
 // terms (detStoL, detLtoS, G != 0) follow the loops.
-#include <cmath>
 #include <mutex>
 #include <vector>
 #include "common.cuh"
@@ -136,11 +135,6 @@ int upload_fop_terms(int device, cudaStream_t st) {
       start[c][p + 1] = (short)flat.size();
     }
   if ((int)flat.size() > MAX_TERMS || (int)tb.disp.size() > MAX_DISP) return -1;
-  // the sign-only kernels rely on |coef| = 1 (U F, F U) and 1/2 (the rest)
-  for (int c = 0; c < NTF; c++)
-    for (int p = 0; p < NPAT; p++)
-      for (const FTerm& T : tb.terms[c][p])
-        if (std::fabs(T.coef) != (p == P_UF || p == P_FU ? 1.0f : 0.5f)) return -1;
   cudaMemcpyToSymbol(c_terms, flat.data(), flat.size() * sizeof(FTerm));
   cudaMemcpyToSymbol(c_pat_start, start, sizeof(start));
   cudaMemcpyToSymbol(c_disp, tb.disp.data(), tb.disp.size() * sizeof(char4));
@@ -184,12 +178,6 @@ SUSY_D unsigned bc_mask(const Geo& g, const Site& c) {
 template <typename R>
 SUSY_D R bc_of(unsigned mask, int dt, R pbc) {
   return ((mask >> (dt + 3)) & 1u) ? pbc : (R)1;
-}
-
-// Sign of a unit-magnitude term as bit 31: the coefficient's sign XOR the
-// temporal BC factor (pneg = 1 when the BC is antiperiodic)
-SUSY_D unsigned term_sign(const FTerm& T, unsigned bcm, unsigned pneg) {
-  return ((__float_as_uint(T.coef) >> 31) ^ ((bcm >> (T.bcdt + 3)) & pneg)) << 31;
 }
 
 // One pattern's terms: compile-time operand fields and adjoints
@@ -400,10 +388,6 @@ SUSY_D double fop_finish(Mat<N, R>& acc, const FopArgs<R>& a, const Site& c, int
   return part;
 }
 
-// One pattern's terms, each added with its sign only: the coefficients of
-// the U F and F U patterns are +-1 and those of F U^dag and U^dag F +-1/2,
-// and the kernel scales the accumulator by 2 before the latter and by 1/2
-// after them (exact), so no product needs a multiply by its coefficient.
 // PP = false: one operand buffer, no prefetch (fewest registers)
 template <int N, typename R, int SIGN, int PAT, bool PP, typename ACC>
 SUSY_D void run_pattern_pp(ACC& acc, const FopArgs<R>& a, int s, unsigned bcm, int t0, int t1) {
@@ -414,7 +398,7 @@ SUSY_D void run_pattern_pp(ACC& acc, const FopArgs<R>& a, int s, unsigned bcm, i
   const int S = a.g.S;
   const typename CT<R>::T* fl = LF ? a.src : a.U;
   const typename CT<R>::T* fr = RF ? a.src : a.U;
-  const unsigned pneg = a.g.pbc < 0 ? 1u : 0u;
+  const R pbc = (R)a.g.pbc;
   if (t0 >= t1) return;
   if (!PP) {
 #pragma unroll 1
@@ -422,7 +406,7 @@ SUSY_D void run_pattern_pp(ACC& acc, const FopArgs<R>& a, int s, unsigned bcm, i
       const FTerm T = c_terms[t];
       const Mat<N, R> L = ldm<N, R, AL>(fl, T.kl, a.nbrtab[(size_t)T.dl * S + s], S);
       const Mat<N, R> Rm = ldm<N, R, AR>(fr, T.kr, a.nbrtab[(size_t)T.dr * S + s], S);
-      acc.add_sign(term_sign(T, bcm, pneg), L, Rm);
+      acc.add((R)T.coef * bc_of<R>(bcm, T.bcdt, pbc), L, Rm);
     }
     return;
   }
@@ -439,7 +423,7 @@ SUSY_D void run_pattern_pp(ACC& acc, const FopArgs<R>& a, int s, unsigned bcm, i
       LB = ldm<N, R, AL>(fl, TB.kl, a.nbrtab[(size_t)TB.dl * S + s], S);
       RB = ldm<N, R, AR>(fr, TB.kr, a.nbrtab[(size_t)TB.dr * S + s], S);
     }
-    acc.add_sign(term_sign(TA, bcm, pneg), LA, RA);
+    acc.add((R)TA.coef * bc_of<R>(bcm, TA.bcdt, pbc), LA, RA);
     if (!hb) break;
     const bool ha = t + 2 < t1;
     if (ha) {
@@ -447,7 +431,7 @@ SUSY_D void run_pattern_pp(ACC& acc, const FopArgs<R>& a, int s, unsigned bcm, i
       LA = ldm<N, R, AL>(fl, TA.kl, a.nbrtab[(size_t)TA.dl * S + s], S);
       RA = ldm<N, R, AR>(fr, TA.kr, a.nbrtab[(size_t)TA.dr * S + s], S);
     }
-    acc.add_sign(term_sign(TB, bcm, pneg), LB, RB);
+    acc.add((R)TB.coef * bc_of<R>(bcm, TB.bcdt, pbc), LB, RB);
     if (!ha) break;
   }
 }
@@ -468,10 +452,8 @@ fermion_op_pp_kernel(FopArgs<R> a) {
     acc.zero();
     run_pattern_pp<N, R, SIGN, P_UF, PP>(acc, a, s, bcm, c_pat_start[comp][0], c_pat_start[comp][1]);
     run_pattern_pp<N, R, SIGN, P_FU, PP>(acc, a, s, bcm, c_pat_start[comp][1], c_pat_start[comp][2]);
-    acc.scale((R)2);
     run_pattern_pp<N, R, SIGN, P_FUD, PP>(acc, a, s, bcm, c_pat_start[comp][2], c_pat_start[comp][3]);
     run_pattern_pp<N, R, SIGN, P_UDF, PP>(acc, a, s, bcm, c_pat_start[comp][3], c_pat_start[comp][4]);
-    acc.scale((R)0.5);
     Mat<N, R> out = acc.get();
     part = fop_finish<N, R, SIGN>(out, a, c, comp);
   }
