@@ -170,6 +170,16 @@ int susy_b200_cg_blocked(susy_b200_lattice *h, int on);
  * one by one.  Same kernels, same results.  on < 0 only queries; returns
  * the previous setting. */
 int susy_b200_use_graphs(susy_b200_lattice *h, int on);
+/* Trajectory pseudofermion solves (no reference counterpart; the reference
+ * solves them one after the other, update_o.c:98-113): on = 1 (default)
+ * with Nroot >= 2 the odd pseudofermions' solves run on a second solver
+ * context of the handle (its own stream and scratch, about as much device
+ * memory again as one solve's fields; made on first use) from a second host
+ * thread while the calling thread runs the even ones, so the solves overlap
+ * on the GPU; on = 0 solves them in turn on the handle's stream.  Same
+ * kernels on the same data: the same results.  on < 0 only queries;
+ * returns the previous setting. */
+int susy_b200_pf_streams(susy_b200_lattice *h, int on);
 /* Solver behind susy_b200_congrad_multi (the host-array drop-in for
  * congrad_multi.c:26): SUSY_B200_SOLVER_FP64 (default, the reference's
  * recurrences) or SUSY_B200_SOLVER_MIXED (same FP64 true-residual bound).

@@ -167,6 +167,54 @@ double* partials(susy_b200_lattice* h, int which) {
 
 long tf_complex(const susy_b200_lattice* h) { return (long)NTF * mat_c(h) * h->g.S; }
 
+// The handle's second solver context, made on first use: its own stream,
+// multi-shift state and scratch fields (allocated as its solves need them);
+// the links, their derived fields in both precisions and the neighbour
+// table are the handle's, which the solvers only read.  The settings the
+// solvers read are copied from the handle at every call.
+susy_b200_lattice* solver_shadow(susy_b200_lattice* h) {
+  if (!h->shadow) {
+    susy_b200_lattice* c = new susy_b200_lattice();
+    c->prm = h->prm;
+    c->g = h->g;
+    c->N = h->N;
+    c->shares_fields = true;
+    if (cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
+      cudaGetLastError();
+      delete c;
+      return nullptr;
+    }
+    c->stream = c->own_stream;
+    c->ms = (MsState*)dalloc(c, sizeof(MsState));
+    if (!c->ms) {
+      susy_b200_destroy(c);
+      return nullptr;
+    }
+    h->shadow = c;
+  }
+  susy_b200_lattice* c = h->shadow;
+  c->U = h->U;
+  c->Uinv = h->Uinv;
+  c->pd = h->pd;
+  c->U32 = h->U32;
+  c->Uinv32 = h->Uinv32;
+  c->pd32 = h->pd32;
+  c->nbrtab = h->nbrtab;
+  c->prm = h->prm;
+  c->G = h->G;
+  c->ms_blocked = h->ms_blocked;
+  c->use_graphs = h->use_graphs;
+  c->mix_switch = h->mix_switch;
+  c->mix_reliable = h->mix_reliable;
+  c->mix_correct32 = h->mix_correct32;
+  for (int pi = 0; pi < 2; pi++) {
+    c->fop_variant[pi] = h->fop_variant[pi];
+    for (int v = 0; v < SUSY_B200_FOP_NVARIANTS; v++) c->fop_ms[pi][v] = h->fop_ms[pi][v];
+  }
+  c->err = 0;
+  return c;
+}
+
 }  // namespace susy
 
 // ===========================================================================
@@ -245,6 +293,9 @@ susy_b200_lattice* susy_b200_create(const susy_b200_params* p) {
 void susy_b200_destroy(susy_b200_lattice* h) {
   if (!h) return;
   cudaStreamSynchronize(h->stream);
+  if (h->shadow) susy_b200_destroy(h->shadow);
+  if (h->shares_fields)  // a solver context: these belong to its handle
+    h->U = h->Uinv = h->pd = h->U32 = h->Uinv32 = h->pd32 = nullptr, h->nbrtab = nullptr;
   void* ptrs[] = {h->U, h->mom, h->Uinv, h->force, h->det, h->pd, h->zw, h->D, h->F,
                   h->U32, h->Uinv32, h->pd32, h->stage, h->ms, h->bigpart, h->gen, h->prn,
                   h->rng_bad, h->ptrbuf, h->nbrtab, h->meas};
@@ -321,6 +372,13 @@ int susy_b200_use_graphs(susy_b200_lattice* h, int on) {
   if (!h) return SUSY_B200_EINVAL;
   const int prev = h->use_graphs;
   if (on >= 0) h->use_graphs = on ? 1 : 0;
+  return prev;
+}
+
+int susy_b200_pf_streams(susy_b200_lattice* h, int on) {
+  if (!h) return SUSY_B200_EINVAL;
+  const int prev = h->pf_streams;
+  if (on >= 0) h->pf_streams = on ? 1 : 0;
   return prev;
 }
 

@@ -5,6 +5,7 @@
 // takes the Metropolis decision.
 #include <cmath>
 #include <cstring>
+#include <thread>
 #include <vector>
 #include "lattice.h"
 #include "hmc.h"
@@ -234,6 +235,84 @@ int solve(susy_b200_lattice* h, const susy_b200_rhmc* r, const void* src, void* 
   return rc ? rc : it;
 }
 
+// The Nroot pseudofermion solves of one force evaluation
+// (update_o.c:169-176, 98-100, 111-113).  With two or more pseudofermions
+// the odd ones run on the handle's second solver context (solver_shadow:
+// own stream, scratch and solver state; links and derived fields shared)
+// from a second host thread while this thread runs the even ones, so two
+// multi-shift solves overlap on the GPU and each one's single-block scalar
+// kernels and launch gaps fill with the other's operator kernels.  Each
+// solve is the same kernel sequence on the same data either way: the
+// solutions are identical to solving one after the other.  Returns the
+// summed iterations or an error.
+static int solve_pfs(susy_b200_lattice* h, const susy_b200_rhmc* r,
+                     const std::vector<void*>& gsrc, std::vector<std::vector<void*>>& psim,
+                     const double* shifts) {
+  const int Nroot = r->Nroot;
+  susy_b200_lattice* c = nullptr;
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+  if (Nroot > 1 && h->pf_streams) {
+    // the operator autotuner times kernels: it runs before the solves overlap
+    if (h->fop_variant[0] < 0) autotune_fop(h, 64);
+    if (r->solver == SUSY_B200_SOLVER_MIXED && h->fop_variant[1] < 0) autotune_fop(h, 32);
+    c = solver_shadow(h);
+    if (c && (cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming) != cudaSuccess ||
+              cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming) != cudaSuccess)) {
+      cudaGetLastError();
+      c = nullptr;
+    }
+  }
+  int total = 0;
+  if (c) {
+    // the context's stream starts after everything issued on the handle's
+    cudaEventRecord(ev[0], h->stream);
+    cudaStreamWaitEvent(c->stream, ev[0], 0);
+    int odd_total = 0, odd_rc = 0, even_rc = 0;
+    bool threaded = true;
+    auto odd = [&]() {
+      for (int n = 1; n < Nroot; n += 2) {
+        const int it = solve(c, r, gsrc[n], psim[n].data(), shifts);
+        if (it < 0) {
+          odd_rc = it;
+          return;
+        }
+        odd_total += it;
+      }
+    };
+    std::thread t;
+    try {
+      t = std::thread(odd);
+    } catch (...) {
+      threaded = false;
+    }
+    for (int n = 0; n < Nroot && !even_rc; n += 2) {
+      const int it = solve(h, r, gsrc[n], psim[n].data(), shifts);
+      if (it < 0)
+        even_rc = it;
+      else
+        total += it;
+    }
+    if (threaded)
+      t.join();
+    else
+      odd();
+    // and the handle's stream continues after the context's solves
+    cudaEventRecord(ev[1], c->stream);
+    cudaStreamWaitEvent(h->stream, ev[1], 0);
+    cudaEventDestroy(ev[0]);
+    cudaEventDestroy(ev[1]);
+    if (even_rc) return even_rc;
+    if (odd_rc) return set_err(h, odd_rc);
+    return total + odd_total;
+  }
+  for (int n = 0; n < Nroot; n++) {
+    const int it = solve(h, r, gsrc[n], psim[n].data(), shifts);
+    if (it < 0) return it;
+    total += it;
+  }
+  return total;
+}
+
 int dev_grsource(susy_b200_lattice* h, const susy_b200_rhmc* r, void* src, int* iters) {
   int rc = dev_gaussian_tf(h, src);
   if (rc) return rc;
@@ -355,10 +434,8 @@ int dev_update(susy_b200_lattice* h, const susy_b200_rhmc* r, susy_b200_traj* re
     for (int n = 0; n < Nroot; n++)
       if ((rc = susy_b200_tf_upload(h, gsrc[n], 64, src_in[n]))) return rc;
   // psim = (D^dag D + shift4)^-1 gsrc   (update_o.c:169-176)
-  for (int n = 0; n < Nroot; n++) {
-    if ((it = solve(h, r, gsrc[n], psim[n].data(), r->shift4)) < 0) return it;
-    iters += it;
-  }
+  if ((it = solve_pfs(h, r, gsrc, psim, r->shift4)) < 0) return it;
+  iters += it;
   double start = 0.0, end = 0.0;
   if ((rc = action_total(h, r, gsrc.data(), pp.data(), res->start_parts, &start))) return rc;
   const size_t b5 = field_bytes(h, 5, 64);
@@ -383,19 +460,17 @@ int dev_update(susy_b200_lattice* h, const susy_b200_rhmc* r, susy_b200_traj* re
     if ((rc = gauge_step(h, r, g_eps, &x))) return rc;
     gnorm += x;
     if (x > max_gf) max_gf = x;
-    for (int n = 0; n < Nroot; n++) {
-      if ((it = solve(h, r, gsrc[n], psim[n].data(), r->shift4)) < 0) return it;
-      iters += it;
+    if ((it = solve_pfs(h, r, gsrc, psim, r->shift4)) < 0) return it;
+    iters += it;
+    for (int n = 0; n < Nroot; n++)
       if ((rc = ff(n, f_eps * LAMBDA_MID))) return rc;
-    }
     if ((rc = gauge_step(h, r, g_eps, &x))) return rc;
     gnorm += x;
     if (x > max_gf) max_gf = x;
-    for (int n = 0; n < Nroot; n++) {
-      if ((it = solve(h, r, gsrc[n], psim[n].data(), r->shift4)) < 0) return it;
-      iters += it;
+    if ((it = solve_pfs(h, r, gsrc, psim, r->shift4)) < 0) return it;
+    iters += it;
+    for (int n = 0; n < Nroot; n++)
       if ((rc = ff(n, f_eps * (i < r->nsteps[0] ? TWO_LAMBDA : LAMBDA)))) return rc;
-    }
   }
   if ((rc = action_total(h, r, gsrc.data(), pp.data(), res->end_parts, &end))) return rc;
   double change = end - start;

@@ -54,6 +54,12 @@ struct susy_b200_lattice {
   void* ptrbuf = nullptr;     // device copy of field pointers / coefficients
   std::vector<void*> gsrc, gr_psim, traj_psim, extra5, refine;
   susy::HostPrn node_prn = {};
+  // second solver context (hmc.cu solve_pfs): its own stream, solver state
+  // and scratch; the links, derived fields and neighbour table are this
+  // handle's (shares_fields set in the context)
+  susy_b200_lattice* shadow = nullptr;
+  bool shares_fields = false;
+  int pf_streams = 1;         // overlap the pseudofermion solves of a trajectory
   int fop_variant[2] = {-1, -1};  // chosen operator kernel (FP64, FP32); -1 = tune
   float fop_ms[2][SUSY_B200_FOP_NVARIANTS] = {};  // autotuner timings per variant
   int err = 0, cuda_err = 0;
@@ -75,6 +81,7 @@ void* scratch_tf(susy_b200_lattice* h, int which, int prec);
 double* partials(susy_b200_lattice* h, int which);
 long tf_complex(const susy_b200_lattice* h);
 void* sol_field(susy_b200_lattice* h, int j);
+susy_b200_lattice* solver_shadow(susy_b200_lattice* h);
 int multishift_fp64(susy_b200_lattice* h, const void* src, void* const* psim, int norder,
                     const double* shift, int MaxCG, double errormin, double* size_r,
                     int* iters);

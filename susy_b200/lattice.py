@@ -162,6 +162,8 @@ def load_library(path: str = LIB_PATH):
     L.susy_b200_set_solver.argtypes = [_vp, C.c_int]
     L.susy_b200_use_graphs.restype = C.c_int
     L.susy_b200_use_graphs.argtypes = [_vp, C.c_int]
+    L.susy_b200_pf_streams.restype = C.c_int
+    L.susy_b200_pf_streams.argtypes = [_vp, C.c_int]
     L.susy_b200_cg_blocked.restype = C.c_int
     L.susy_b200_cg_blocked.argtypes = [_vp, C.c_int]
     L.susy_b200_dev_congrad_multi.argtypes = [_vp, _vp, C.POINTER(_vp), C.c_int, _dp, C.c_int,
@@ -476,6 +478,11 @@ class Lattice:
         """CUDA-graph replay (1) or plain launches (0) of the solver's
         iteration chunks; returns the previous setting."""
         return self._check(self.lib.susy_b200_use_graphs(self.h, int(on)))
+
+    def pf_streams(self, on: int = -1) -> int:
+        """Overlap the pseudofermion solves of a trajectory on two streams
+        (1) or solve them in turn (0); returns the previous setting."""
+        return self._check(self.lib.susy_b200_pf_streams(self.h, int(on)))
 
     def cg_blocked(self, on: int = -1) -> int:
         """Blocked (1) or per-iteration (0) vector update of the FP64

@@ -279,3 +279,27 @@ def test_update_batch_equals_one_by_one():
     for g, w in zip(got, want):
         assert g["accept"] == w["accept"] and g["iters"] == w["iters"]
         assert g["delta_S"] == w["delta_S"] and g["start"] == w["start"]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("solver", [0, 1])
+def test_overlapped_pseudofermion_solves_give_the_same_trajectory(solver):
+    """Nroot = 2: the two pseudofermions' solves overlapped on two streams
+    (the default) give exactly the trajectory of solving them in turn, with
+    the FP64 and with the mixed solver, over two trajectories in a row."""
+    dims, N = (4, 4, 4, 8), 2
+    def run(pf):
+        lat = Lattice(dims, N, pbc=-1, lam=1.0, bmass=0.2, G=0.05, iseed=21)
+        lat.set_links(synth.to_ref(dims, synth.links(dims, N, 0.2, 22)))
+        lat.fop_variant(64, 8)
+        lat.fop_variant(32, 9)
+        assert lat.pf_streams(pf) == 1
+        r = RHMC(15, 2, nstep=3, nstep_gauge=2, traj_length=0.5, error_per_site=1e-8,
+                 solver=solver)
+        res = [lat.update(r) for _ in range(2)]
+        return res, lat.get_links()
+    (a, la), (b, lb) = run(1), run(0)
+    for x, y in zip(a, b):
+        assert x["iters"] == y["iters"] and x["accept"] == y["accept"]
+        assert x["delta_S"] == y["delta_S"] and x["start"] == y["start"]
+    assert np.array_equal(la, lb)
