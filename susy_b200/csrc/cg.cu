@@ -61,6 +61,7 @@ __global__ void k_ms_init(MsState* st, const double* partials, int np, int maxcg
     st->skip = (st->rsq <= st->rsqstop || maxcg <= 0) ? 1 : 0;
     st->skip_b = 1;
     st->record = record;
+    st->done_r = 0;
     st->blk_len = 0;
     st->blk_start = 0;
     for (int j = 0; j < MS_MAXS; j++) st->live[j] = j < st->nshift;
@@ -105,11 +106,12 @@ __global__ void k_ms_scalars1(MsState* st, const double* partials, int np) {
   }
 }
 
-__global__ void k_ms_scalars2(MsState* st, const double* partials, int np) {
-  __shared__ double sh[ST];
-  if (st->skip) return;
+// The scalar recurrences after the residual update, run by one block of ST
+// threads: its own kernel, or the last block of the fused residual update
+// (partials read from L2: other blocks wrote them)
+SUSY_D void scalars2_block(MsState* st, const double* partials, int np, double* sh) {
   double v = 0.0;
-  for (int i = threadIdx.x; i < np; i += ST) v += partials[i];
+  for (int i = threadIdx.x; i < np; i += ST) v += __ldcg(partials + i);
   const double rsqnew = block_reduce_all(v, sh);
   if (threadIdx.x != 0) return;
   const double a0 = rsqnew / st->rsq;
@@ -148,6 +150,12 @@ __global__ void k_ms_scalars2(MsState* st, const double* partials, int np) {
     st->zeta_i[j] = st->zeta_ip1[j];
   }
   st->skip = (rsqnew <= st->rsqstop || st->iter >= st->maxcg) ? 1 : 0;
+}
+
+__global__ void k_ms_scalars2(MsState* st, const double* partials, int np) {
+  __shared__ double sh[ST];
+  if (st->skip) return;
+  scalars2_block(st, partials, np, sh);
 }
 
 // psi_j -= beta_j p_j (j = 0 and every live shift), r += beta_0 mp, |r|^2
@@ -420,10 +428,18 @@ void ms_update_p0(MsState* st, const MsVecs& v, int prec, long n, cudaStream_t s
 
 // r(i) = r(i-1) + beta_0 mp and partials of |r(i)|^2; i = iteration count
 // after this iteration's scalars1.  MT: type of mp (FP64, or FP32 when the
-// operator ran in FP32)
+// operator ran in FP32).  The block that finishes last (a counter in the
+// solver state, taken after each block's partial is written and fenced)
+// sums the partials and runs the scalar recurrences, which saves a
+// dependent single-block launch per iteration; it resets the counter for
+// the next launch.  Every block reads skip before the last one can change
+// it.
 template <typename MT>
 __global__ void __launch_bounds__(UT) k_msb_update_r(MsState* st, MsBlockVecs v, long n,
                                                      double* part) {
+  static_assert(UT == ST, "the last block runs the ST-thread scalar step");
+  __shared__ double sh[ST];
+  __shared__ int last;
   if (st->skip) return;
   const int it = st->iter;
   const double b0 = st->beta_i[0];
@@ -441,7 +457,15 @@ __global__ void __launch_bounds__(UT) k_msb_update_r(MsState* st, MsBlockVecs v,
     acc += r.x * r.x + r.y * r.y;
   }
   acc = block_sum<UT>(acc);
-  if (threadIdx.x == 0) part[blockIdx.x] = acc;
+  if (threadIdx.x == 0) {
+    part[blockIdx.x] = acc;
+    __threadfence();
+    last = atomicAdd(&st->done_r, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!last) return;
+  if (threadIdx.x == 0) st->done_r = 0;
+  scalars2_block(st, part, gridDim.x, sh);
 }
 
 // p0 = r(i) + alpha_0 p0 (and its FP32 copy for an FP32 operator)
@@ -599,14 +623,13 @@ __global__ void k_msb_block_reset(MsState* st) {
 
 // Returns the number of partials written (at most 8 blocks per SM of a
 // 148-SM B200)
-int msb_update_r(MsState* st, const MsBlockVecs& v, long n, double* part, bool mp32,
-                 cudaStream_t s) {
+void msb_update_r(MsState* st, const MsBlockVecs& v, long n, double* part, bool mp32,
+                  cudaStream_t s) {
   const int nb = vec_blocks(n) < 1184 ? vec_blocks(n) : 1184;
   if (mp32)
     count_launch(), k_msb_update_r<float2><<<nb, UT, 0, s>>>(st, v, n, part);
   else
     count_launch(), k_msb_update_r<double2><<<nb, UT, 0, s>>>(st, v, n, part);
-  return nb;
 }
 
 // Residual replacement: r(k) <- rt with the matching search-vector

@@ -21,7 +21,8 @@ struct MsState {
   // (hb = beta_j, 0 once shift j is frozen; hz = zeta_j(i+1); ha = alpha_j),
   // iterations recorded so far, iteration count at the block start, and
   // the shifts still live when the block began
-  int record, blk_len, blk_start, pad2;
+  int record, blk_len, blk_start;
+  unsigned done_r;    // blocks of the fused residual update finished so far
   int live[MS_MAXS];
   double hb[MS_BLK][MS_MAXS], hz[MS_BLK][MS_MAXS], ha[MS_BLK][MS_MAXS];
   double shift[MS_MAXS];
@@ -121,8 +122,10 @@ void ms_update_p0(MsState* st, const MsVecs& v, int prec, long n, cudaStream_t s
 void norm2_partials(const void* x, int prec, long n, double* part, cudaStream_t s);
 int rdot_partials(long n, const void* a, const void* b, double* part, cudaStream_t s);
 void copy_field(long n, const void* a, void* b, cudaStream_t s);
-int msb_update_r(MsState* st, const MsBlockVecs& v, long n, double* part, bool mp32,
-                 cudaStream_t s);
+// r(i) = r(i-1) + beta_0 mp, then (in the kernel's last block) the scalar
+// recurrences of ms_scalars2 on |r(i)|^2
+void msb_update_r(MsState* st, const MsBlockVecs& v, long n, double* part, bool mp32,
+                  cudaStream_t s);
 void msb_replace(MsState* st, const MsBlockVecs& v, long n, const void* rt, double rsq,
                  cudaStream_t s);
 void msb_update_p0(MsState* st, const MsBlockVecs& v, long n, cudaStream_t s);

@@ -257,8 +257,7 @@ static int ms_run_block(susy_b200_lattice* h, const void* src, void* const* psim
         np_fop = dev_fop(h, tmp, mp, -1, 64, p0, fm2 + shift[0], part0, skip);
       }
       ms_scalars1(h->ms, part0, np_fop, s);
-      const int np_r = msb_update_r(h->ms, v, n, part1, fp32_op, s);
-      ms_scalars2(h->ms, part1, np_r, s);
+      msb_update_r(h->ms, v, n, part1, fp32_op, s);
       msb_update_p0(h->ms, v, n, s);
       if ((k + 1) % MS_BLK == 0) msb_block(h->ms, v, n, s);
     }
