@@ -186,7 +186,7 @@ int susy_b200_pf_streams(susy_b200_lattice *h, int on);
  * Returns the previous setting. */
 int susy_b200_set_solver(susy_b200_lattice *h, int solver);
 /* Mixed-precision solver settings (no reference counterpart): the operator
- * runs in FP32 once |r| < fp32_below |src| (default 3e-4); with the FP32
+ * runs in FP32 once |r| < fp32_below |src| (default 3e-5); with the FP32
  * operator the FP64 true residual replaces the iterated one whenever |r|
  * fell by reliable_factor (default 1e-2) since the last replacement.
  * 0 < fp32_below <= 1, 0 < reliable_factor < 1, else SUSY_B200_EINVAL. */

@@ -40,7 +40,7 @@ struct susy_b200_lattice {
   int ms_blocked = 1;         // FP64 multi-shift CG: blocked vector update
   int use_graphs = 1;         // replay the solver's iteration chunks as CUDA graphs
   int host_solver = 0;        // solver behind susy_b200_congrad_multi
-  double mix_switch = 3e-4;   // mixed solver: FP32 operator once |r| < this |src|
+  double mix_switch = 3e-5;   // mixed solver: FP32 operator once |r| < this |src|
   double mix_reliable = 1e-2; // mixed solver: true residual when |r| fell this much
   int mix_correct32 = 1;      // mixed solver: per-shift corrections with the FP32 operator
   std::vector<void*> extra;   // other lazily allocated fields

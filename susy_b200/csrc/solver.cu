@@ -2,7 +2,7 @@
 //
 // multishift_fp64   the reference's congrad_multi in FP64 throughout.
 // multishift_mixed  (1) the same multi-shift recurrences (blocked update)
-//                   with the operator in FP32 once |r| < 3e-4 |src| and
+//                   with the operator in FP32 once |r| < 3e-5 |src| and
 //                   FP64 reliable updates of the base residual;
 //                   (2) per shift, the FP64 true residual
 //                   r = b - (D^dag D + sigma) x; a shift with
@@ -170,7 +170,7 @@ static double true_residual(susy_b200_lattice* h, const void* b, const void* x, 
 //
 // mixed = false: FP64 throughout (the reference's solver).
 // mixed = true: the operator runs in FP64 until |r| < mix_switch |src|
-// (handle setting, default 3e-4) and in FP32 after that; every vector,
+// (handle setting, default 3e-5) and in FP32 after that; every vector,
 // the recurrences and the solutions stay FP64.  Once the operator is FP32,
 // the iterated residual drifts from the true one by the FP32 rounding of
 // each product, so at block boundaries, whenever |r| fell by mix_reliable
@@ -182,7 +182,10 @@ static double true_residual(susy_b200_lattice* h, const void* b, const void* x, 
 // which never see a residual replacement, keep an error of order FP32
 // rounding times that residual.  Switching earlier costs more in the
 // per-shift correction solves than it saves: measured at 12^3 x 24 U(3),
-// switching at 1e-3 took 894 iterations in all, at 3e-4 588 (FP64: 567).
+// switching at 1e-3 took 894 iterations in all, at 3e-4 588 (FP64: 567);
+// in full trajectories, whose solves run ~2200 iterations, the corrections
+// after a switch at 3e-4 cost more than the FP32 operator saved, and 3e-5
+// was the fastest of 3e-4 ... 1e-5.
 
 static int ms_run_block(susy_b200_lattice* h, const void* src, void* const* psim, int norder,
                         const double* shift, int MaxCG, double errormin, bool mixed,

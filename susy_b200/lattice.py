@@ -431,7 +431,7 @@ class Lattice:
     def autotune(self):
         self._check(self.lib.susy_b200_autotune(self.h))
 
-    def mixed_params(self, fp32_below: float = 3e-4, reliable_factor: float = 1e-2):
+    def mixed_params(self, fp32_below: float = 3e-5, reliable_factor: float = 1e-2):
         """Mixed solver: FP32 operator once |r| < fp32_below |src|; FP64
         residual replacement whenever |r| fell by reliable_factor."""
         self._check(self.lib.susy_b200_mixed_params(self.h, float(fp32_below),
