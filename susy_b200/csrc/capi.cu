@@ -167,6 +167,25 @@ double* partials(susy_b200_lattice* h, int which) {
 
 long tf_complex(const susy_b200_lattice* h) { return (long)NTF * mat_c(h) * h->g.S; }
 
+// Stream and event of the host congrad_multi's early solution copies
+cudaStream_t copy_stream(susy_b200_lattice* h) {
+  if (!h->copy) {
+    cudaStream_t st = nullptr;
+    if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) {
+      cudaGetLastError();
+      return nullptr;
+    }
+    if (cudaEventCreateWithFlags(&h->copy_ev, cudaEventDisableTiming) != cudaSuccess) {
+      cudaGetLastError();
+      h->copy_ev = nullptr;
+      cudaStreamDestroy(st);
+      return nullptr;
+    }
+    h->copy = st;
+  }
+  return h->copy;
+}
+
 // The handle's second solver context, made on first use: its own stream,
 // multi-shift state and scratch fields (allocated as its solves need them);
 // the links, their derived fields in both precisions and the neighbour
@@ -312,6 +331,8 @@ void susy_b200_destroy(susy_b200_lattice* h) {
     for (void* p : *v)
       if (p) cudaFree(p);
   if (h->poll) cudaFreeHost(h->poll);
+  if (h->copy) cudaStreamSynchronize(h->copy), cudaStreamDestroy(h->copy);
+  if (h->copy_ev) cudaEventDestroy(h->copy_ev);
   if (h->own_stream) cudaStreamDestroy(h->own_stream);
   delete h;
 }
@@ -615,14 +636,41 @@ int susy_b200_congrad_multi(susy_b200_lattice* h, const double* src, double* con
     ps[j] = sol_field(h, j);
     if (!ps[j]) return SUSY_B200_ENOMEM;
   }
+  // When every psim[j] is page-locked host memory, a shift's solution goes
+  // back (layout change into the staging buffer, then the copy) on a second
+  // stream as soon as the shift has frozen, while the solve continues; the
+  // rest, and any the mixed solver corrected afterwards, follow the solve.
+  // Pageable buffers would make the copies block the host, so they wait.
+  bool early = copy_stream(h) != nullptr;
+  for (int j = 0; j < norder && early; j++) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, psim[j]) != cudaSuccess || a.type != cudaMemoryTypeHost) {
+      cudaGetLastError();
+      early = false;
+    }
+  }
+  const size_t bytes = (size_t)h->g.V * NTF * mat_c(h) * 2 * sizeof(double);
+  std::vector<char> sent(norder, 0), redo(norder, 0);
+  FrozenHook hook = [&](int j) {
+    cudaEventRecord(h->copy_ev, h->stream);
+    cudaStreamWaitEvent(h->copy, h->copy_ev, 0);
+    soa_to_aos(h->g, NTF, h->N, ps[j], h->stage, 64, h->copy);
+    cudaMemcpyAsync(psim[j], h->stage, bytes, cudaMemcpyDeviceToHost, h->copy);
+    sent[j] = 1;
+  };
   int it = 0;
   double sr = 0.0;
   r = h->host_solver == SUSY_B200_SOLVER_MIXED
-          ? multishift_mixed(h, s, ps.data(), norder, shift, MaxCG, errormin, &sr, &it)
-          : multishift_fp64(h, s, ps.data(), norder, shift, MaxCG, errormin, &sr, &it);
+          ? multishift_mixed(h, s, ps.data(), norder, shift, MaxCG, errormin, &sr, &it,
+                             early ? &hook : nullptr, redo.data())
+          : multishift_fp64(h, s, ps.data(), norder, shift, MaxCG, errormin, &sr, &it,
+                            early ? &hook : nullptr);
+  // the early copies finish before the staging buffer is used again
+  if (early && !ck(h, cudaStreamSynchronize(h->copy))) return SUSY_B200_ECUDA;
   if (r) return r;
   for (int j = 0; j < norder; j++)
-    if ((r = susy_b200_tf_download(h, ps[j], 64, psim[j]))) return r;
+    if (!sent[j] || redo[j])
+      if ((r = susy_b200_tf_download(h, ps[j], 64, psim[j]))) return r;
   if (size_r) *size_r = sr;
   return it;
 }

@@ -1,5 +1,6 @@
 // Internal definition of the opaque handle declared in include/susy_b200.h.
 #pragma once
+#include <functional>
 #include <vector>
 #include "../../include/susy_b200.h"
 #include "kernels.h"
@@ -60,6 +61,8 @@ struct susy_b200_lattice {
   susy_b200_lattice* shadow = nullptr;
   bool shares_fields = false;
   int pf_streams = 1;         // overlap the pseudofermion solves of a trajectory
+  cudaStream_t copy = nullptr;   // host congrad_multi: early solution copies
+  cudaEvent_t copy_ev = nullptr;
   int fop_variant[2] = {-1, -1};  // chosen operator kernel (FP64, FP32); -1 = tune
   float fop_ms[2][SUSY_B200_FOP_NVARIANTS] = {};  // autotuner timings per variant
   int err = 0, cuda_err = 0;
@@ -82,9 +85,14 @@ double* partials(susy_b200_lattice* h, int which);
 long tf_complex(const susy_b200_lattice* h);
 void* sol_field(susy_b200_lattice* h, int j);
 susy_b200_lattice* solver_shadow(susy_b200_lattice* h);
+cudaStream_t copy_stream(susy_b200_lattice* h);
+// Called by the blocked solver at a poll for each shift j >= 1 whose
+// solution the multi-shift pass has finished (the shift froze and its last
+// block pass ran): the host API copies it out while the solve goes on
+typedef std::function<void(int)> FrozenHook;
 int multishift_fp64(susy_b200_lattice* h, const void* src, void* const* psim, int norder,
                     const double* shift, int MaxCG, double errormin, double* size_r,
-                    int* iters);
+                    int* iters, const FrozenHook* on_frozen = nullptr);
 int measure(susy_b200_lattice* h, susy_b200_meas* m);
 int net_apply(susy_b200_net* n, const void* src, void* dst);
 int multishift_learned(susy_b200_lattice* h, susy_b200_net* net, const void* src,

@@ -34,7 +34,7 @@ static void* pvec(susy_b200_lattice* h, int j, int prec) {
 
 static int* poll_words(susy_b200_lattice* h) {
   if (!h->poll) {
-    if (cudaMallocHost(&h->poll, 4 * sizeof(int)) != cudaSuccess) {
+    if (cudaMallocHost(&h->poll, (4 + MS_MAXS) * sizeof(int)) != cudaSuccess) {
       cudaGetLastError();
       h->poll = nullptr;
     }
@@ -189,7 +189,8 @@ static double true_residual(susy_b200_lattice* h, const void* b, const void* x, 
 
 static int ms_run_block(susy_b200_lattice* h, const void* src, void* const* psim, int norder,
                         const double* shift, int MaxCG, double errormin, bool mixed,
-                        double* size_r, int* iters, double errormin_base = -1.0) {
+                        double* size_r, int* iters, double errormin_base = -1.0,
+                        const FrozenHook* on_frozen = nullptr) {
   cudaStream_t s = h->stream;
   const long n = tf_complex(h);
   const size_t bv = field_bytes(h, NTF, 64);
@@ -244,6 +245,7 @@ static int ms_run_block(susy_b200_lattice* h, const void* src, void* const* psim
     rsqstop = errormin * bnorm;
   }
   int launched = 0, replacements = 0;
+  std::vector<char> handed(norder, 0);
   // SUSY_B200_CG_TRACE=1 prints the solver's progress at every poll (stderr)
   static const bool trace = [] {
     const char* e = getenv("SUSY_B200_CG_TRACE");
@@ -284,7 +286,16 @@ static int ms_run_block(susy_b200_lattice* h, const void* src, void* const* psim
     cudaMemcpyAsync(pw, &h->ms->skip, sizeof(int), cudaMemcpyDeviceToHost, s);
     cudaMemcpyAsync(pw + 1, &h->ms->iter, sizeof(int), cudaMemcpyDeviceToHost, s);
     cudaMemcpyAsync(pd, &h->ms->rsq, sizeof(double), cudaMemcpyDeviceToHost, s);
+    if (on_frozen)
+      cudaMemcpyAsync(pw + 4, h->ms->converged, norder * sizeof(int), cudaMemcpyDeviceToHost, s);
     if (!ck(h, cudaStreamSynchronize(s))) return SUSY_B200_ECUDA;
+    // a shift frozen by now had its last block pass at this block boundary
+    if (on_frozen)
+      for (int j = 1; j < norder; j++)
+        if (pw[4 + j] && !handed[j]) {
+          handed[j] = 1;
+          (*on_frozen)(j);
+        }
     bool stop = pw[0] != 0;
     if (trace)
       fprintf(stderr, "susy_b200 cg: it %d rsq %.6e rel %.3e stop %d fp32 %d\n", pw[1], *pd,
@@ -332,9 +343,10 @@ static int ms_run_block(susy_b200_lattice* h, const void* src, void* const* psim
 // Reference-faithful FP64 multi-shift CG (congrad_multi.c:26-221)
 int multishift_fp64(susy_b200_lattice* h, const void* src, void* const* psim, int norder,
                     const double* shift, int MaxCG, double errormin, double* size_r,
-                    int* iters) {
+                    int* iters, const FrozenHook* on_frozen) {
   if (h->ms_blocked)
-    return ms_run_block(h, src, psim, norder, shift, MaxCG, errormin, false, size_r, iters);
+    return ms_run_block(h, src, psim, norder, shift, MaxCG, errormin, false, size_r, iters,
+                        -1.0, on_frozen);
   return ms_run(h, src, psim, norder, shift, MaxCG, errormin, 64, 64, size_r, iters);
 }
 
@@ -360,17 +372,20 @@ static double true_residual(susy_b200_lattice* h, const void* b, const void* x, 
 
 int multishift_mixed(susy_b200_lattice* h, const void* src, void* const* psim, int norder,
                      const double* shift, int MaxCG, double errormin, double* size_r,
-                     int* iters) {
+                     int* iters, const FrozenHook* on_frozen, char* redo) {
   const long n = tf_complex(h);
   int it1 = 0, rc;
   double sr = 0.0;
   // (1) multi-shift pass, FP32 operator once the residual is small; should
   // the FP32 phase fail (a non-finite value, or the iterated residual
   // running away from the true one), the plain FP64 solve replaces it
-  rc = ms_run_block(h, src, psim, norder, shift, MaxCG, errormin, true, &sr, &it1);
+  rc = ms_run_block(h, src, psim, norder, shift, MaxCG, errormin, true, &sr, &it1, -1.0,
+                    on_frozen);
   if (rc == SUSY_B200_ENOCONV || rc == SUSY_B200_ENAN) {
     cudaStreamSynchronize(h->stream);
     h->err = 0;
+    if (redo)
+      for (int j = 0; j < norder; j++) redo[j] = 1;
     int it64 = 0;
     rc = ms_run_block(h, src, psim, norder, shift, MaxCG, errormin, false, &sr, &it64);
     it1 += it64;
@@ -409,6 +424,7 @@ int multishift_mixed(susy_b200_lattice* h, const void* src, void* const* psim, i
                     &it2);
       if (rc) return rc;
       total += it2;
+      if (redo) redo[j] = 1;
       axpy_field(n, 1.0, e64, psim[j], h->stream);
       const double before = rr;
       rr = true_residual(h, src, psim[j], shift[j], r64, r32);

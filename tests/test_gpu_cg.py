@@ -175,3 +175,28 @@ def test_mixed_corrections_meet_bound(fp32):
         y = ref[j].download()
         assert np.abs(x - y).max() <= 1e-8 * np.abs(y).max()
     assert lat.lib.susy_b200_mixed_correction(lat.h, 2) < 0
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("solver", [0, 1])
+def test_host_congrad_multi_early_copies(solver):
+    """susy_b200_congrad_multi into page-locked host buffers hands each
+    frozen shift's solution back while the solve continues: the solutions
+    are the ones pageable buffers get (copied after the solve), with the
+    FP64 and the mixed solver."""
+    import torch
+    dims, N = (8, 8, 8, 8), 2
+    lat = Lattice(dims, N, pbc=-1, lam=1.0, bmass=0.2, G=0.05)
+    lat.set_links(synth.to_ref(dims, synth.links(dims, N, 0.2, 1)))
+    lat.set_solver(solver)
+    shifts = synth.geometric_shifts(15, 1e-5, 1e3)
+    src = synth.to_ref(dims, synth.tf_source(dims, N, 62))
+    pinned = [torch.empty(lat.tf_doubles, dtype=torch.float64, pin_memory=True).numpy()
+              for _ in shifts]
+    pageable = [np.empty(lat.tf_doubles) for _ in shifts]
+    for outs in (pinned, pageable):
+        for o in outs:
+            o[:] = np.nan
+        lat.congrad_multi(src, outs, shifts, 20000, 1e-20)
+    for a, b in zip(pinned, pageable):
+        assert np.array_equal(a, b)
