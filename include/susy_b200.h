@@ -206,7 +206,7 @@ int susy_b200_dev_DSq(susy_b200_lattice *h, const void *src, void *dst, int prec
  * buffer themselves and must not have a library call cudaMalloc (an
  * application with its own device memory pool, or code that cannot afford
  * the device-wide synchronisation an allocation may cause): no handle is
- * needed and nothing is allocated, not even on the first call.  All
+ * needed and the library calls no allocation routine.  All
  * pointers are FP64 device fields in the device layout (structure of
  * arrays, lexicographic sites x + nx (y + ny (z + nz t)), site stride
  * S = volume rounded up to a multiple of 32, complex {re, im} doubles):
@@ -219,8 +219,14 @@ int susy_b200_dev_DSq(susy_b200_lattice *h, const void *src, void *dst, int prec
  * for any ncol); larger lattices return SUSY_B200_ESCRATCH.  Every call on
  * a device shares that array: calls whose kernels overlap on the GPU (other
  * streams, other host threads) race and must be serialised by the caller.
- * The first call on each device looks up the array's device address, so
- * make that first call before any stream capture.  Launches on cuda_stream
+ * The library's modules load lazily: the first call on each device loads
+ * this one, and the driver reserves the 16 MiB array at that moment (with
+ * whatever synchronisation a module load implies).  Make that first call at
+ * set-up time, before any stream capture.  Every call looks the array's
+ * device address up again, so a cudaDeviceReset in between is harmless.
+ * Extents must be even and >= 2 and ncol 2..4 (else SUSY_B200_EINVAL);
+ * the volume is formed in 64 bits, so extents whose product would wrap a
+ * 32-bit int return SUSY_B200_ESCRATCH.  Launches on cuda_stream
  * (NULL = default stream) and returns without synchronising. */
 int susy_b200_DSq_noalloc(int nx, int ny, int nz, int nt, int ncol, int pbc, double G,
                           double fmass, const void *links, const void *Uinv,

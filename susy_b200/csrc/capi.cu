@@ -6,6 +6,7 @@
 #include <cmath>
 #include <vector>
 #include <atomic>
+#include <climits>
 #include "../../include/susy_b200.h"
 #include "kernels.h"
 #include "lattice.h"
@@ -30,6 +31,31 @@ void count_launches(long long n) {
 long long thread_launch_count() { return t_launches; }
 
 static size_t mat_c(const susy_b200_lattice* h) { return (size_t)h->N * h->N; }
+
+bool make_geo(long nx, long ny, long nz, long nt, int ncol, int pbc, Geo* g) {
+  if (ncol < 2 || ncol > 4 || (pbc != 1 && pbc != -1)) return false;
+  const long ext[4] = {nx, ny, nz, nt};
+  for (long e : ext)
+    if (e < 2 || (e & 1) || e > INT_MAX) return false;
+  // Each factor is below 2^31, so the products are checked step by step
+  // against the bound before they can leave the 64-bit range.
+  const long lim = INT_MAX / (NTF * (long)ncol * ncol);
+  long V = 1;
+  for (long e : ext) {
+    if (V > lim / e) return false;
+    V *= e;
+  }
+  const long S = (V + 31) / 32 * 32;
+  if ((long)NTF * ncol * ncol * S > INT_MAX) return false;
+  g->nx = (int)nx;
+  g->ny = (int)ny;
+  g->nz = (int)nz;
+  g->nt = (int)nt;
+  g->V = (int)V;
+  g->S = (int)S;
+  g->pbc = pbc;
+  return true;
+}
 
 bool ck(susy_b200_lattice* h, cudaError_t e) {
   if (e == cudaSuccess) return true;
@@ -240,11 +266,8 @@ susy_b200_lattice* solver_shadow(susy_b200_lattice* h) {
 extern "C" {
 
 susy_b200_lattice* susy_b200_create(const susy_b200_params* p) {
-  // Even extents >= 2: the reference's parity-ordered site layout
-  // (layout_hyper_prime.c:157-170) is a bijection only then.
-  if (!p || p->ncol < 2 || p->ncol > 4 || p->nx < 2 || p->ny < 2 || p->nz < 2 || p->nt < 2 ||
-      (p->nx | p->ny | p->nz | p->nt) & 1 || (p->pbc != 1 && p->pbc != -1))
-    return nullptr;
+  Geo geo;
+  if (!p || !make_geo(p->nx, p->ny, p->nz, p->nt, p->ncol, p->pbc, &geo)) return nullptr;
   if (cudaSetDevice(p->device) != cudaSuccess) {
     cudaGetLastError();
     return nullptr;
@@ -253,13 +276,7 @@ susy_b200_lattice* susy_b200_create(const susy_b200_params* p) {
   h->prm = *p;
   h->N = p->ncol;
   h->G = p->G;
-  h->g.nx = p->nx;
-  h->g.ny = p->ny;
-  h->g.nz = p->nz;
-  h->g.nt = p->nt;
-  h->g.V = p->nx * p->ny * p->nz * p->nt;
-  h->g.S = (h->g.V + 31) / 32 * 32;
-  h->g.pbc = p->pbc;
+  h->g = geo;
   if (cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
     cudaGetLastError();
     delete h;

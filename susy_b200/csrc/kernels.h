@@ -7,6 +7,14 @@
 
 namespace susy {
 
+// Geometry from lattice extents, checked before anything is sized from it:
+// even extents >= 2 (the reference's parity-ordered site layout,
+// layout_hyper_prime.c:157-170, is a bijection only then), NCOL 2..4, PBC
+// +-1, and the volume computed in 64 bits and bounded so that every 32-bit
+// element index of one Twist_Fermion (16 NCOL^2 S complex) stays below
+// INT_MAX.  Returns false (and leaves g untouched) otherwise.
+bool make_geo(long nx, long ny, long nz, long nt, int ncol, int pbc, Geo* g);
+
 constexpr int MS_MAXS = 32;
 // Iterations per block of the blocked solution/search-vector update
 constexpr int MS_BLK = 8;

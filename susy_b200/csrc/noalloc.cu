@@ -8,7 +8,6 @@
 // the operator without this library ever calling cudaMalloc.  The array is
 // part of the loaded module: every GPU that loads the library holds its
 // 16 MiB until the process exits.
-#include <mutex>
 #include "../../include/susy_b200.h"
 #include "common.cuh"
 #include "kernels.h"
@@ -21,28 +20,19 @@ constexpr long NOALLOC_MAX_COMPLEX = 1L << 20;
 
 static __device__ __align__(256) double2 g_noalloc_tmp[NOALLOC_MAX_COMPLEX];
 
-// Device address of g_noalloc_tmp per device.  In host code the array's name
-// is only a host-side stand-in, so the address comes from
-// cudaGetSymbolAddress, made once per device with that device current.
-static std::mutex g_noalloc_mu;
-static void* g_noalloc_ptr[64];
-
+// Device address of g_noalloc_tmp on the current device.  In host code the
+// array's name is only a host-side stand-in, so the address comes from
+// cudaGetSymbolAddress with the device current.  It is looked up on every
+// call rather than cached: after a cudaDeviceReset the module is loaded
+// again, possibly at another address, and a cached pointer would be stale.
+// Once the module is loaded the lookup is a table search in the runtime.
 static int noalloc_scratch(void** out) {
-  int dev = -1;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+  void* p = nullptr;
+  if (cudaGetSymbolAddress(&p, g_noalloc_tmp) != cudaSuccess || !p) {
     cudaGetLastError();
     return SUSY_B200_ECUDA;
   }
-  std::lock_guard<std::mutex> lk(g_noalloc_mu);
-  if (!g_noalloc_ptr[dev]) {
-    void* p = nullptr;
-    if (cudaGetSymbolAddress(&p, g_noalloc_tmp) != cudaSuccess || !p) {
-      cudaGetLastError();
-      return SUSY_B200_ECUDA;
-    }
-    g_noalloc_ptr[dev] = p;
-  }
-  *out = g_noalloc_ptr[dev];
+  *out = p;
   return SUSY_B200_OK;
 }
 
@@ -54,17 +44,16 @@ extern "C" int susy_b200_DSq_noalloc(int nx, int ny, int nz, int nt, int ncol, i
                                      double fmass, const void* links, const void* Uinv,
                                      const void* plaqdet, const void* src, void* dst,
                                      void* cuda_stream) {
-  if (ncol < 2 || ncol > 4 || nx < 2 || ny < 2 || nz < 2 || nt < 2 ||
-      ((nx | ny | nz | nt) & 1) || (pbc != 1 && pbc != -1))
-    return SUSY_B200_EINVAL;
+  // Extents are checked and the volume formed in 64 bits before anything is
+  // sized from it: a volume that wrapped in int could pass the scratch bound
+  // while the kernels index the caller's fields with the real extents.
   Geo g;
-  g.nx = nx;
-  g.ny = ny;
-  g.nz = nz;
-  g.nt = nt;
-  g.V = nx * ny * nz * nt;
-  g.S = (g.V + 31) / 32 * 32;
-  g.pbc = pbc;
+  if (!make_geo(nx, ny, nz, nt, ncol, pbc, &g)) {
+    const bool shape_ok = ncol >= 2 && ncol <= 4 && nx >= 2 && ny >= 2 && nz >= 2 && nt >= 2 &&
+                          !((nx | ny | nz | nt) & 1) && (pbc == 1 || pbc == -1);
+    // well-formed extents whose volume is only too large: the scratch limit
+    return shape_ok ? SUSY_B200_ESCRATCH : SUSY_B200_EINVAL;
+  }
   if ((long)NTF * ncol * ncol * g.S > NOALLOC_MAX_COMPLEX) return SUSY_B200_ESCRATCH;
   const bool doG = G > 1e-8;
   if (!links || !src || !dst || (doG && (!Uinv || !plaqdet))) return SUSY_B200_EINVAL;

@@ -72,3 +72,25 @@ def test_lattice_without_gpu_raises_loudly():
         pytest.skip("a GPU is present")
     with pytest.raises(L.SusyError):
         L.Lattice((4, 4, 4, 4), 2)
+
+
+def test_create_rejects_extents_whose_volume_overflows_int():
+    """Extents whose product wraps a 32-bit int are refused before anything
+    is sized from them (the wrapped value could look small)."""
+    lib = L.load_library()
+    for dims in ((2, 2, 2048, 524290), (65536, 65536, 2, 2), (1 << 30, 2, 2, 2)):
+        p = L.Params(*dims, 2, -1, 0.5, 0, 0, 0, 0, 41, 0)
+        assert not lib.susy_b200_create(C.byref(p)), dims
+
+
+def test_noalloc_refuses_overflowing_extents_before_any_device_work():
+    lib = L.load_library()
+    f = lib.susy_b200_DSq_noalloc
+    f.restype = C.c_int
+    f.argtypes = [C.c_int] * 6 + [C.c_double, C.c_double] + [C.c_void_p] * 6
+    # 2 x 2 x 2048 x 524290 wraps to 16384 sites in int arithmetic
+    for dims in ((2, 2, 2048, 524290), (65536, 65536, 2, 2), (46342, 46342, 2, 2)):
+        assert f(*dims, 2, -1, 0.0, 0.0, None, None, None, None, None, None) == -6, dims
+    # malformed extents stay invalid arguments
+    assert f(2, 2, 2047, 4, 2, -1, 0.0, 0.0, None, None, None, None, None, None) == -1
+    assert f(-2, 2, 2, 4, 2, -1, 0.0, 0.0, None, None, None, None, None, None) == -1
