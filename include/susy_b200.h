@@ -197,7 +197,7 @@ int susy_b200_mixed_params(susy_b200_lattice *h, double fp32_below, double relia
  * the FP64 true residual is checked after every pass) or in FP64 (fp32 = 0).
  * No counterpart in the reference.  fp32 not 0 or 1: SUSY_B200_EINVAL. */
 int susy_b200_mixed_correction(susy_b200_lattice *h, int fp32);
-#define SUSY_B200_FOP_NVARIANTS 10   /* entries of ms_per_variant */
+#define SUSY_B200_FOP_NVARIANTS 12   /* entries of ms_per_variant */
 int susy_b200_autotune(susy_b200_lattice *h);
 int susy_b200_fop_variant(susy_b200_lattice *h, int prec, int set_to, float *ms_per_variant);
 int susy_b200_dev_DSq(susy_b200_lattice *h, const void *src, void *dst, int prec);

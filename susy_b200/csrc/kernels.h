@@ -81,9 +81,12 @@ struct MsBlockVecs {
 // 12^3x24 U(3): the FP64 optimum is the 128-register site-major kernel
 // (0.215 ms vs 0.260 uncapped; 102 registers: 0.256, 64: 0.59), the FP32 one
 // the 64-register component-major kernel (0.117 ms vs 0.135; 48: 0.166).
+// FOP_SITE_MAJOR_SHN / FOP_COMP_MAJOR_SHN: the _OCC kernels with each
+// block's neighbour indices preloaded into shared memory.
 enum { FOP_MAT = 0, FOP_MAT_CM = 1, FOP_ROWS = 2, FOP_COMPACT = 3, FOP_COMPACT_PF = 4,
        FOP_SITE_MAJOR_PP = 5, FOP_COMP_MAJOR_PP = 6, FOP_SITE_MAJOR = 7,
-       FOP_SITE_MAJOR_OCC = 8, FOP_COMP_MAJOR_OCC = 9, FOP_NVARIANTS = 10 };
+       FOP_SITE_MAJOR_OCC = 8, FOP_COMP_MAJOR_OCC = 9, FOP_SITE_MAJOR_SHN = 10,
+       FOP_COMP_MAJOR_SHN = 11, FOP_NVARIANTS = 12 };
 template <typename R>
 int fermion_op(const Geo& g, int N, const void* U, const void* Uinv, const void* pd,
                 const void* src, void* dst, int sign, double G, const void* add, double addc,

@@ -116,3 +116,29 @@ def test_bad_sign_raises():
         __import__("ctypes").POINTER(__import__("ctypes").c_double)),
         src.ctypes.data_as(__import__("ctypes").POINTER(__import__("ctypes").c_double)), 2)
     assert rc == -1
+
+
+@pytest.mark.parametrize("dims,N,pbc", [((2, 2, 2, 6), 3, -1), ((4, 2, 2, 6), 2, -1),
+                                        ((4, 2, 4, 6), 3, 1)])
+def test_every_variant_where_warps_straddle_time_slices(dims, N, pbc):
+    """With 8 or 16 sites per time slice a 32-site tile spans several time
+    slices, boundary slices included, so the temporal BC sign of a product
+    differs between the lanes of one warp.  Every kernel variant, D and
+    D^dag, FP64 to 1e-13 and FP32 to 1e-5 against the oracle."""
+    from susy_b200.lattice import FOP_NVARIANTS
+    lat, geo, prm, U, der = setup(dims, N, pbc, 0.05)
+    src = synth.tf_source(dims, N, seed=23)
+    a, b = lat.tf(64), lat.tf(64)
+    a32, b32 = lat.tf(32), lat.tf(32)
+    a.upload(synth.to_ref(dims, src))
+    lat.dev_convert(a, a32)
+    for sign in (1, -1):
+        want = O.fermion_op(geo, prm, U, der, src, sign)
+        for v in range(FOP_NVARIANTS):
+            lat.fop_variant(64, v)
+            lat.fop_variant(32, v)
+            lat.dev_fermion_op(a, b, sign)
+            assert rel(synth.from_ref(dims, b.download(), 16, N), want) < FP64_TOL, (v, sign)
+            lat.dev_fermion_op(a32, b32, sign)
+            lat.dev_convert(b32, b)
+            assert rel(synth.from_ref(dims, b.download(), 16, N), want) < FP32_TOL, (v, sign)
