@@ -164,6 +164,12 @@ int susy_b200_plaquette(susy_b200_lattice *h, double *ss_plaq, double *st_plaq);
  * order); on = 0: the per-iteration update.  on < 0 only queries.
  * Returns the previous setting. */
 int susy_b200_cg_blocked(susy_b200_lattice *h, int on);
+/* Iterations each shift of the last multi-shift solve on this handle took
+ * (no reference counterpart; congrad_multi.c:154-165 freezes shift j once
+ * zeta_j^2 |r|^2 <= rsqstop and updates it no more): iters[j] = the
+ * iteration at which shift j froze, the solve's iteration count for the
+ * base shift and for shifts that never froze.  1 <= norder <= 32. */
+int susy_b200_cg_freeze_iterations(susy_b200_lattice *h, int *iters, int norder);
 /* Solver launch mode (no reference counterpart): on = 1 (default) captures
  * the ~100 kernel launches of 16 solver iterations into a CUDA graph once
  * per solve and operator precision and replays it; on = 0 launches them
@@ -379,7 +385,9 @@ int susy_b200_dev_congrad_multi_learned(susy_b200_lattice *h, susy_b200_net *net
 /* Independent lattices at once (no reference counterpart: the reference
  * runs one lattice per process): one update() per handle, h[i] with r[i]
  * into res[i], the handles' streams driven concurrently by `threads` host
- * threads (at most 16).  Each lattice's result is the one update() gives it alone.
+ * threads (at most n).  Each handle's operator kernels are tuned first, one
+ * handle at a time, unless already tuned.  Each lattice's result is the one
+ * update() gives it alone.
  * Returns the total CG iterations or the first negative error code. */
 int susy_b200_update_batch(susy_b200_lattice *const *h, const susy_b200_rhmc *const *r,
                            susy_b200_traj *res, int n, int threads);

@@ -19,6 +19,12 @@
 # default: that build's pseudofermion refresh reads uninitialised memory
 # (grsource.c:79-92) and printed NaN actions on its first trajectory here,
 # so it cannot serve as an oracle.
+# An argument shim<NCOL> (after <NCOL> in the same call or an earlier one)
+# links the reference's susy_hmc once more with susy_b200/shim/b200_shim.c
+# in place of the hot-path functions it replaces, against
+# susy_b200/libsusy_b200.so: the replaced symbols are weakened in copies of
+# the reference objects (objcopy --weaken-symbol), so the shim's strong
+# definitions win at link time; output oracle/_ref/n<NCOL>/susy_hmc_b200.
 # Outputs go only to oracle/_ref/ (git-ignored, shipped with the tree).
 # The reference's own build system is not used.
 set -euo pipefail
@@ -114,7 +120,48 @@ build_one() {
   echo "built $D/susy_hmc and $OUT/libsusyref_n$N$SUF.so"
 }
 
+# fermion_op / DSq (utilities.c), congrad_multi, fermion_force and
+# gauge_force (update_h.c), update_u (update_o.c): taken from the shim
+build_shim() {
+  local N=$1 D=$OUT/n$1
+  local ROOT
+  ROOT=$(cd "$HERE/.." && pwd)
+  if [ ! -e "$D/obj/utilities.o" ]; then
+    echo "build_ref.sh: build NCOL=$N before shim$N" >&2
+    exit 2
+  fi
+  if [ ! -e "$ROOT/susy_b200/libsusy_b200.so" ]; then
+    echo "build_ref.sh: susy_b200/libsusy_b200.so not built" >&2
+    exit 2
+  fi
+  mkdir -p "$D/objw"
+  objcopy --weaken-symbol=fermion_op --weaken-symbol=DSq "$D/obj/utilities.o" "$D/objw/utilities.o"
+  objcopy --weaken-symbol=congrad_multi "$D/obj/congrad_multi.o" "$D/objw/congrad_multi.o"
+  objcopy --weaken-symbol=fermion_force --weaken-symbol=gauge_force "$D/obj/update_h.o" \
+      "$D/objw/update_h.o"
+  objcopy --weaken-symbol=update_u "$D/obj/update_o.o" "$D/objw/update_o.o"
+  ln -sf "$ROOT/susy_b200/shim/b200_shim.c" "$D/susy/zz_b200_shim.c"
+  $CC -c $APP_FLAGS -I"$D/susy" -I"$ROOT/include" "$D/susy/zz_b200_shim.c" -o "$D/objw/b200_shim.o"
+  local objs=()
+  for f in "$D"/obj/*.o; do
+    local b
+    b=$(basename "$f")
+    case "$b" in
+      control.o|ref_harness.o|lapack_min.o) continue ;;
+      utilities.o|congrad_multi.o|update_h.o|update_o.o) objs+=("$D/objw/$b") ;;
+      *) objs+=("$f") ;;
+    esac
+  done
+  $CC -o "$D/susy_hmc_b200" "$D/obj/control.o" "${objs[@]}" "$D/objw/b200_shim.o" \
+      "$D/obj/lapack_min.o" -L"$ROOT/susy_b200" -lsusy_b200 \
+      -Wl,-rpath,'$ORIGIN/../../../susy_b200' -lm
+  echo "built $D/susy_hmc_b200"
+}
+
 mkdir -p "$OUT"
 for N in "${NCOLS[@]}"; do
-  build_one "$N"
+  case "$N" in
+    shim*) build_shim "${N#shim}" ;;
+    *) build_one "$N" ;;
+  esac
 done

@@ -24,9 +24,20 @@ extern "C" int susy_b200_update_batch(susy_b200_lattice* const* hs,
   if (!hs || !rs || !res || n < 0) return SUSY_B200_EINVAL;
   for (int i = 0; i < n; i++)
     if (!hs[i] || !rs[i]) return SUSY_B200_EINVAL;
-  // at most 16 host threads: the configuration measured; one run with 48
-  // threads ended in a host crash whose cause was not found
-  const int nt = std::max(1, std::min(std::min(threads > 0 ? threads : 1, n), 16));
+  // Every handle's operator kernels are tuned here, one handle after the
+  // other on this thread with the GPU otherwise idle, before any worker
+  // starts: tuned inside the workers, each handle would time its kernels
+  // against the other lattices' work (noise for picks) and allocate its
+  // tuning fields while other workers capture their solver graphs.
+  for (int i = 0; i < n; i++) {
+    if (cudaSetDevice(hs[i]->prm.device) != cudaSuccess) return SUSY_B200_ECUDA;
+    for (int prec : {64, 32}) {
+      if (hs[i]->fop_variant[prec == 64 ? 0 : 1] >= 0) continue;
+      const int rt = autotune_fop(hs[i], prec);
+      if (rt < 0) return rt;
+    }
+  }
+  const int nt = std::max(1, std::min(threads > 0 ? threads : 1, n));
   std::atomic<int> next(0);
   std::vector<int> rc(n, 0);
   auto work = [&]() {

@@ -427,6 +427,19 @@ int susy_b200_cg_blocked(susy_b200_lattice* h, int on) {
   return prev;
 }
 
+int susy_b200_cg_freeze_iterations(susy_b200_lattice* h, int* iters, int norder) {
+  if (!h || !iters || norder < 1 || norder > MS_MAXS) return SUSY_B200_EINVAL;
+  std::vector<int> c(norder, 0), n(1, 0);
+  if (!ck(h, cudaMemcpyAsync(c.data(), h->ms->converged, norder * sizeof(int),
+                             cudaMemcpyDeviceToHost, h->stream)) ||
+      !ck(h, cudaMemcpyAsync(n.data(), &h->ms->iter, sizeof(int), cudaMemcpyDeviceToHost,
+                             h->stream)) ||
+      !ck(h, cudaStreamSynchronize(h->stream)))
+    return SUSY_B200_ECUDA;
+  for (int j = 0; j < norder; j++) iters[j] = j == 0 || c[j] == 0 ? n[0] : c[j];
+  return SUSY_B200_OK;
+}
+
 int susy_b200_last_error(const susy_b200_lattice* h) { return h ? h->err : SUSY_B200_EINVAL; }
 
 const char* susy_b200_error_string(int code) {

@@ -141,7 +141,8 @@ SUSY_D void scalars2_block(MsState* st, const double* partials, int np, double* 
   st->rsq = rsqnew;
   for (int j = 1; j < st->nshift; j++) {
     if (st->converged[j]) continue;
-    if (rsqnew * st->zeta_ip1[j] * st->zeta_ip1[j] <= st->rsqfreeze) st->converged[j] = 1;
+    // converged[j] = the iteration at which shift j froze (>= 1; 0 = live)
+    if (rsqnew * st->zeta_ip1[j] * st->zeta_ip1[j] <= st->rsqfreeze) st->converged[j] = st->iter;
   }
   for (int j = 0; j < st->nshift; j++) {
     if (st->converged[j]) continue;

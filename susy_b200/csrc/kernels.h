@@ -36,7 +36,8 @@ struct MsState {
   double shift[MS_MAXS];
   double zeta_i[MS_MAXS], zeta_im1[MS_MAXS], zeta_ip1[MS_MAXS];
   double beta_i[MS_MAXS], beta_im1[MS_MAXS], alpha[MS_MAXS];
-  int converged[MS_MAXS], active_p[MS_MAXS];
+  int converged[MS_MAXS];   // 0 while shift j is live, else the iteration it froze at
+  int active_p[MS_MAXS];
   // p_j update deferred to the next iteration's vector pass:
   // p_j <- pz_j r + pa_j p_j when pact_j
   double pz[MS_MAXS], pa[MS_MAXS];

@@ -166,6 +166,8 @@ def load_library(path: str = LIB_PATH):
     L.susy_b200_pf_streams.argtypes = [_vp, C.c_int]
     L.susy_b200_cg_blocked.restype = C.c_int
     L.susy_b200_cg_blocked.argtypes = [_vp, C.c_int]
+    L.susy_b200_cg_freeze_iterations.restype = C.c_int
+    L.susy_b200_cg_freeze_iterations.argtypes = [_vp, C.POINTER(C.c_int), C.c_int]
     L.susy_b200_dev_congrad_multi.argtypes = [_vp, _vp, C.POINTER(_vp), C.c_int, _dp, C.c_int,
                                               C.c_double, _dp, C.POINTER(C.c_int)]
     L.susy_b200_dev_congrad_multi_mixed.argtypes = [_vp, _vp, C.POINTER(_vp), C.c_int, _dp,
@@ -488,6 +490,13 @@ class Lattice:
         """Blocked (1) or per-iteration (0) vector update of the FP64
         multi-shift CG; returns the previous setting (on < 0 only queries)."""
         return self._check(self.lib.susy_b200_cg_blocked(self.h, int(on)))
+
+    def cg_freeze_iterations(self, norder: int) -> list:
+        """Iteration at which each shift of the last multi-shift solve froze
+        (the solve's iteration count for the base shift)."""
+        out = (C.c_int * norder)()
+        self._check(self.lib.susy_b200_cg_freeze_iterations(self.h, out, int(norder)))
+        return list(out)
 
     def fop_variant(self, prec: int = 64, set_to: int = -1):
         """(current variant, autotuner ms per variant) for one precision."""

@@ -33,6 +33,44 @@ def lattice_from_ops(d):
     return lat, dims, N
 
 
+def test_u3_operator_matches_reference_on_8x8x8x16():
+    """fermion_op(+1), fermion_op(-1) and DSq on an 8^3 x 16 U(3) lattice
+    against the reference operator (tests/golden/ops_U3_8x8x8x16.npz, made
+    by tests/golden/make_golden_u3_large.py from seeded inputs regenerated
+    here): every FP64 kernel variant, 256 sampled sites (both temporal
+    boundaries included) to 1e-13 relative, whole-lattice |out|^2 and four
+    weighted projections to 1e-12 relative."""
+    import importlib.util
+    from susy_b200.lattice import FOP_NVARIANTS
+    spec = importlib.util.spec_from_file_location(
+        "mg", os.path.join(GOLD, "make_golden_u3_large.py"))
+    mg = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mg)
+    f = np.load(os.path.join(GOLD, "ops_U3_8x8x8x16.npz"))
+    dims, N = tuple(int(x) for x in f["dims"]), int(f["N"])
+    lat = Lattice(dims, N, pbc=-1, lam=2.0, bmass=0.3, G=0.05)
+    lat.set_links(synth.to_ref(dims, synth.links(dims, N, 0.2, mg.LINK_SEED)))
+    src = synth.to_ref(dims, synth.tf_source(dims, N, mg.SRC_SEED))
+    out = np.zeros(lat.tf_doubles)
+
+    def check(name):
+        at, n2, pj = mg.summarise(out, f["sites"])
+        want = f[name]
+        assert rel(at, want) < 1e-13, name
+        assert abs(n2 - float(f["norm2_" + name])) < 1e-12 * float(f["norm2_" + name]), name
+        assert np.abs(pj - f["proj_" + name]).max() < 1e-12 * np.abs(f["proj_" + name]).max()
+
+    for v in range(FOP_NVARIANTS):
+        lat.fop_variant(64, v)
+        lat.fermion_op(src, out, 1)
+        check("fop_plus")
+        lat.fermion_op(src, out, -1)
+        check("fop_minus")
+    lat.autotune()
+    lat.DSq(src, out)
+    check("DSq")
+
+
 @pytest.mark.parametrize("N", [2, 3])
 def test_cuda_matches_reference_vectors(N):
     d = dict(np.load(os.path.join(GOLD, "ops_U%d.npz" % N)))
@@ -124,13 +162,17 @@ def test_cuda_reproduces_hmc_regression_output(N):
         assert not mismatches(got_lines, want)
 
 
-def test_mixed_solver_keeps_the_accept_decisions():
+@pytest.mark.parametrize("N", [2, 3])
+def test_mixed_solver_keeps_the_accept_decisions(N):
     """The mixed-precision solver reaches the same FP64 true-residual bound,
-    so the trajectories and accept/reject decisions stay those of the golden."""
-    gold, got = run_hmc_ref(2, SOLVER_MIXED)
+    so the trajectories, accept/reject decisions and delta S are those of
+    the golden to the tolerances the FP64 solver meets."""
+    gold, got = run_hmc_ref(N, SOLVER_MIXED)
     for g, t in zip(got, gold["trajectories"]):
         assert g["accept"] == t["accept"]
-        assert abs(g["delta_S"] - t["delta_S"]) <= 0.05
+        assert abs(g["start"] - t["start_S"]) < 1e-6
+        assert abs(g["end"] - t["end_S"]) < 1e-6
+        assert abs(g["delta_S"] - t["delta_S"]) <= 1e-3 * max(abs(t["delta_S"]), 1e-3)
 
 
 def test_smd_with_full_refresh_is_the_hmc_regression_run():

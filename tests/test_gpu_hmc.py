@@ -159,6 +159,46 @@ def test_reversibility():
     assert abs(a["delta_S"] + b["delta_S"]) < 1e-6
 
 
+def test_reversibility_mixed_solver():
+    """The reversibility test with the mixed-precision solver at the FP64
+    true residual 1e-10 per site: links and momenta return to 1e-8, and
+    the forward and backward delta S cancel."""
+    dims, N = (4, 4, 4, 4), 3
+    lat, geo, prm, U = make(dims, N, noise=0.1, seed=6, lam=1.0, bmass=0.2, G=0.05)
+    r = RHMC(15, 1, nstep=3, nstep_gauge=2, traj_length=0.6, error_per_site=1e-10,
+             solver=SOLVER_MIXED, no_metropolis=True)
+    U0 = lat.get_links()
+    mom0 = synth.to_ref(dims, synth.links(dims, N, 0.5, 21) - np.eye(N))
+    src = [synth.to_ref(dims, synth.tf_source(dims, N, 22, 0.3))]
+    a = lat.update_replay(r, mom0, src)
+    P1 = lat.get_mom()
+    b = lat.update_replay(r, -P1, src)
+    assert np.abs(lat.get_links() - U0).max() < 1e-8
+    assert np.abs(lat.get_mom() + mom0).max() < 1e-8
+    assert abs(a["delta_S"] + b["delta_S"]) < 1e-6
+
+
+@pytest.mark.parametrize("N", [2, 3])
+def test_mixed_and_fp64_integrate_the_same_trajectory(N):
+    """Same start links, momenta and pseudofermion sources, error_per_site
+    1e-10: the trajectory with the mixed-precision solver ends where the
+    FP64 one does (links to 1e-9, delta S to 1e-7 absolute)."""
+    dims = (4, 4, 4, 8)
+    lat, geo, prm, U = make(dims, N, noise=0.15, seed=8, lam=1.0, bmass=0.2, G=0.05)
+    U0 = lat.get_links()
+    mom0 = synth.to_ref(dims, synth.links(dims, N, 0.5, 23) - np.eye(N))
+    src = [synth.to_ref(dims, synth.tf_source(dims, N, 24, 0.3)) for _ in range(2)]
+    out = {}
+    for name, solver in (("fp64", SOLVER_FP64), ("mixed", SOLVER_MIXED)):
+        lat.set_links(U0)
+        r = RHMC(15, 2, nstep=4, nstep_gauge=2, traj_length=1.0, error_per_site=1e-10,
+                 solver=solver, no_metropolis=True)
+        res = lat.update_replay(r, mom0, src)
+        out[name] = (res, lat.get_links())
+    assert np.abs(out["mixed"][1] - out["fp64"][1]).max() < 1e-9
+    assert abs(out["mixed"][0]["delta_S"] - out["fp64"][0]["delta_S"]) < 1e-7
+
+
 @pytest.mark.parametrize("N", [2, 3])
 def test_mixed_solver_reaches_fp64_residual(N):
     dims = (4, 4, 4, 8)
@@ -275,6 +315,32 @@ def test_update_batch_equals_one_by_one():
     rh = [RHMC(15, 1, nstep=3, nstep_gauge=2, traj_length=0.5, error_per_site=1e-6)
           for _ in specs]
     got = update_batch(build(), rh, threads=4)
+    want = [lat.update(r) for lat, r in zip(build(), rh)]
+    for g, w in zip(got, want):
+        assert g["accept"] == w["accept"] and g["iters"] == w["iters"]
+        assert g["delta_S"] == w["delta_S"] and g["start"] == w["start"]
+
+
+def test_update_batch_with_more_threads_than_sixteen():
+    """24 lattices on 24 host threads (one per lattice; the pool once had a
+    16-thread cap): every lattice's trajectory is exactly its solo one."""
+    from susy_b200 import update_batch
+    vols = [(4, 4, 4, 4), (2, 2, 2, 4), (4, 4, 2, 4), (2, 4, 2, 4)]
+
+    def build():
+        out = []
+        for i in range(24):
+            dims = vols[i % len(vols)]
+            lat = Lattice(dims, 2, pbc=-1, lam=[0.5, 1.0, 2.0, 4.0][i % 4], bmass=0.2, G=0.05,
+                          iseed=100 + i)
+            lat.set_links(synth.to_ref(dims, synth.links(dims, 2, 0.1 + 0.01 * i, 60 + i)))
+            lat.fop_variant(64, 3)
+            lat.fop_variant(32, 3)
+            out.append(lat)
+        return out
+    rh = [RHMC(15, 1, nstep=2, nstep_gauge=2, traj_length=0.5, error_per_site=1e-6)
+          for _ in range(24)]
+    got = update_batch(build(), rh, threads=24)
     want = [lat.update(r) for lat, r in zip(build(), rh)]
     for g, w in zip(got, want):
         assert g["accept"] == w["accept"] and g["iters"] == w["iters"]

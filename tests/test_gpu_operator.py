@@ -142,3 +142,44 @@ def test_every_variant_where_warps_straddle_time_slices(dims, N, pbc):
             lat.dev_fermion_op(a32, b32, sign)
             lat.dev_convert(b32, b)
             assert rel(synth.from_ref(dims, b.download(), 16, N), want) < FP32_TOL, (v, sign)
+
+
+@pytest.mark.parametrize("N", [2, 3])
+def test_links_and_momenta_in_place_with_a_site_stride(N):
+    """The reference keeps link[5] and mom[5] inside its per-site struct
+    (susy/lattice.h:29-59) and would hand &lattice[0].link[0] with stride
+    sizeof(site).  Emulate that with a padded record per site (links and
+    momenta at odd offsets inside a record much larger than them, bytes in
+    between filled with a marker): set_links / set_mom read the strided
+    fields, the operator matches the contiguous upload, and get_links /
+    get_mom write back into the records without touching the bytes between
+    them."""
+    import ctypes as C
+    dims = (4, 4, 2, 6)
+    lat, geo, prm, U, der = setup(dims, N, -1, 0.05)
+    V = lat.V
+    m5 = 5 * N * N * 2                              # doubles in link[5]
+    rec = 8 * (3 * m5 + 37)                         # bytes per site record
+    off_link, off_mom = 8 * 11, 8 * (11 + m5 + 17)
+    links = synth.to_ref(dims, U)
+    mom = synth.to_ref(dims, synth.links(dims, N, 0.4, 12) - np.eye(N))
+    buf = np.full(V * rec // 8, -7.25)
+    view = buf.reshape(V, rec // 8)
+    view[:, off_link // 8: off_link // 8 + m5] = links.reshape(V, m5)
+    view[:, off_mom // 8: off_mom // 8 + m5] = mom.reshape(V, m5)
+    dp = C.POINTER(C.c_double)
+    base = buf.ctypes.data
+    lib = lat.lib
+    assert lib.susy_b200_set_links(lat.h, C.cast(base + off_link, dp), rec) == 0
+    assert lib.susy_b200_set_mom(lat.h, C.cast(base + off_mom, dp), rec) == 0
+    src = synth.tf_source(dims, N, seed=41)
+    out = np.zeros(lat.tf_doubles)
+    lat.fermion_op(synth.to_ref(dims, src), out, 1)
+    want = O.fermion_op(geo, prm, U, der, src, 1)
+    assert rel(synth.from_ref(dims, out, 16, N), want) < FP64_TOL
+    assert np.array_equal(lat.get_mom(), mom)
+    # write back into fresh records: the fields land in place, the rest stays
+    back = np.full_like(buf, -7.25)
+    assert lib.susy_b200_get_links(lat.h, C.cast(back.ctypes.data + off_link, dp), rec) == 0
+    assert lib.susy_b200_get_mom(lat.h, C.cast(back.ctypes.data + off_mom, dp), rec) == 0
+    assert np.array_equal(back, buf)

@@ -172,3 +172,29 @@ def test_measurements_on_the_regression_start_config(N):
     U = cfg["links"].astype(np.complex128)
     m = O.measurements(geo, prm, U, O.compute_derived(geo, prm, U))
     assert not mismatches(printed(m, geo.V), gold["start_meas"])
+
+
+def test_oracle_operator_matches_reference_on_8x8x8x16_u3():
+    """The numpy restatement against the reference operator on the 8^3 x 16
+    U(3) fixture (sampled sites to 1e-13 relative, whole-lattice norms and
+    weighted projections to 1e-12)."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location(
+        "mg", os.path.join(GOLD, "make_golden_u3_large.py"))
+    mg = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mg)
+    f = np.load(os.path.join(GOLD, "ops_U3_8x8x8x16.npz"))
+    dims, N = tuple(int(x) for x in f["dims"]), int(f["N"])
+    geo = O.Geometry(dims, -1)
+    prm = O.Params(lam=2.0, bmass=0.3, G=0.05, N=N)
+    U = synth.links(dims, N, 0.2, mg.LINK_SEED)
+    der = O.compute_derived(geo, prm, U)
+    src = synth.tf_source(dims, N, mg.SRC_SEED)
+    for name, val in (("fop_plus", O.fermion_op(geo, prm, U, der, src, 1)),
+                      ("fop_minus", O.fermion_op(geo, prm, U, der, src, -1))):
+        at, n2, pj = mg.summarise(synth.to_ref(dims, val), f["sites"])
+        want = f[name]
+        assert np.abs(at - want).max() / np.abs(want).max() < 1e-13, name
+        assert abs(n2 - float(f["norm2_" + name])) < 1e-12 * float(f["norm2_" + name]), name
+        wp = f["proj_" + name]
+        assert np.abs(pj - wp).max() < 1e-12 * np.abs(wp).max(), name
