@@ -1,27 +1,34 @@
 """Benchmark of the RHMC fermion path on B200.
 
 Workload (the metric's configuration): 12^3 x 24 lattice, U(3) (NCOL = 3),
-lambda = 2, bmass = 0.3, G = 0.05, antiperiodic temporal BC; links seeded
-near the identity (noise 0.1, unthermalised); one multi-shift CG solve of
-the degree-15 RHMC system with Nroot = 2 (the 15 shift4 poles of
-setup_rhmc.c) on a complex-Gaussian Twist_Fermion source, to an FP64 true
-residual |r|^2 <= 1e-20 |src|^2 (error_per_site 1e-10).  One "step" is one
-such solve.  Inputs are resident in HBM when the timed region starts; the
-working set (~3 GB) is larger than L2, so no flush is needed.
+lambda = 2, bmass = 0.3, G = 0.05, antiperiodic temporal BC, on the links
+of configs/thermalised_12x12x12x24_u3.lat (identity + 0.1 noise, seed 11,
+thermalised by 20 RHMC trajectories of this integrator: configs/
+thermalise.py; the file's checksums are verified and reported).  One
+"step" is one multi-shift CG solve of the degree-15 RHMC system with
+Nroot = 2 (the 15 shift4 poles of setup_rhmc.c) on a complex-Gaussian
+Twist_Fermion source, to an FP64 true residual |r|^2 <= 1e-20 |src|^2
+(error_per_site 1e-10).  Inputs are resident in HBM when the timed region
+starts; the working set (~3 GB) is larger than L2, so no flush is needed.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--solver mixed|fp64]
+                  [--solver mixed|fp64] [--no-traj]
 
 The timed solver is the mixed one by default (FP64 operator until
 |r| < 3e-5 |src|, FP32 operator after, FP64 residual replacement and
 per-shift FP64 check: the same FP64 true-residual bound as the FP64 solver,
 reported as true_residual_rel_max); the FP64 solver of the reference's
 recurrences is timed right after it in the same run (fp64_s_per_solve).
+On one GPU the line also carries one full RHMC trajectory per solver (15 x
+3 steps, the same start links and random numbers for both): s_per_traj,
+delta S, acceptance and CG iterations.
 
 N > 1 runs one independent replica per GPU (torchrun, NCCL only for the
 barrier and the max-over-ranks time): "value" is the whole-job seconds per
 solve, max rank time / (K * N).  The reference arm times the reference's own
-CPU congrad_multi (oracle/_ref) on a bounded sample of the same solve.
+CPU congrad_multi (oracle/_ref) on bounded samples of the same solve,
+weighted by the solve's recorded schedule of live shifts
+(configs/solve_profile_12x12x12x24_u3.json).
 """
 from __future__ import annotations
 
@@ -48,14 +55,38 @@ TRAJ_SEED = 13
 NORDER, NROOT = 15, 2
 ERRORMIN = 1e-20          # error_per_site 1e-10 squared (setup.c:356-359)
 MAXCG = 20000
-# Iterations the FP64 multi-shift solve of this seeded input takes (the
-# reference runs the identical recurrence); used to extrapolate the
-# reference arm's bounded sample to one full solve.
-REF_ITERS = 567
 REF_SAMPLE_ITERS = 2
+# live-shift counts the reference arm samples (cycled over its steps); its
+# per-iteration cost is fitted as a + b * (live shifts)
+REF_SAMPLE_SHIFTS = (1, 8, 15)
+REF_SAMPLE_TIMEOUT = 600   # seconds one sample (set-up of the replicas included) may take
 METRIC = "s/RHMC traj & CG solve time, 12^3x24 U(3): FP32+learned vs FP64 @1e-10 resid"
 WORKLOAD = ("12^3x24 U(3) multi-shift CG solve, Norder 15 / Nroot 2 shift4 poles, "
-            "FP64 true residual 1e-10 per site")
+            "FP64 true residual 1e-10 per site, thermalised links")
+LINKS_FILE = os.path.join(ROOT, "configs", "thermalised_12x12x12x24_u3.lat")
+PROFILE_FILE = os.path.join(ROOT, "configs", "solve_profile_12x12x12x24_u3.json")
+
+
+def workload_links():
+    """The benchmark links in the reference host layout and the file's
+    header facts; raises if the file is absent or its checksums fail."""
+    from susy_b200 import io_lat, synth
+    dims, ncol, links, info = io_lat.read_gauge(LINKS_FILE)
+    if tuple(dims) != DIMS or ncol != NCOL:
+        raise RuntimeError("%s holds a %s U(%d) lattice" % (LINKS_FILE, dims, ncol))
+    if not info["checksum_ok"]:
+        raise RuntimeError("checksum mismatch in " + LINKS_FILE)
+    info["checksums"] = "%x %x" % (info["sum29"], info["sum31"])
+    return synth.to_ref(DIMS, links), info
+
+
+def bench_config(extra=None):
+    """config keys shared by both arms."""
+    c = {"workload": WORKLOAD, "lattice": "12x12x12x24", "ncol": NCOL, "lambda": LAM,
+         "bmass": BMASS, "G": G, "norder": NORDER, "nroot": NROOT,
+         "links": "configs/thermalised_12x12x12x24_u3.lat"}
+    c.update(extra or {})
+    return c
 
 
 def algorithmic_bytes_fop(V, N, w, doG=True):
@@ -137,44 +168,47 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------------------
-def reference_cpu_samples(nsamples: int, iters: int):
-    """Time nsamples runs of `iters` iterations of the reference's
-    congrad_multi on the bench workload, each from the zero initial guess
-    (runs in the calling process: a worker of cpu_samples)."""
-    from oracle.ref_ctypes import RefLattice
+_REF = {}
+
+
+def _ref_init(kind):
+    """Pool worker set-up: one reference lattice (or the numpy port's
+    fields) on the workload links, kept for all of this worker's samples."""
     from susy_b200 import synth
     from susy_b200.rhmc_tables import rhmc
-    ref = RefLattice(NCOL, dims=DIMS, pbc=-1, lam=LAM, bmass=BMASS, G=G, Nroot=NROOT,
-                     Norder=NORDER)
-    ref.set_links(synth.to_ref(DIMS, synth.links(DIMS, NCOL, LINK_NOISE, LINK_SEED)))
-    ref.compute_all()
+    links, _ = workload_links()
     src = synth.to_ref(DIMS, synth.tf_source(DIMS, NCOL, SRC_SEED))
-    shifts = np.array(rhmc(NORDER, NROOT)["shift4"])
-    out = []
-    for _ in range(nsamples):
-        t0 = time.perf_counter()
-        _, it, _ = ref.congrad_multi(src, shifts, iters, ERRORMIN)
-        out.append((time.perf_counter() - t0, it))
-    return out
+    _REF["shifts"] = np.array(rhmc(NORDER, NROOT)["shift4"])
+    _REF["kind"] = kind
+    if kind == "reference":
+        from oracle.ref_ctypes import RefLattice
+        ref = RefLattice(NCOL, dims=DIMS, pbc=-1, lam=LAM, bmass=BMASS, G=G, Nroot=NROOT,
+                         Norder=NORDER)
+        ref.set_links(links)
+        ref.compute_all()
+        _REF["ref"], _REF["src"] = ref, src
+    else:
+        from oracle import susy_np as O
+        geo = O.Geometry(DIMS, -1)
+        prm = O.Params(lam=LAM, bmass=BMASS, G=G, N=NCOL)
+        U = synth.from_ref(DIMS, links, 5, NCOL)
+        _REF["port"] = (geo, prm, U, O.compute_derived(geo, prm, U))
+        _REF["src"] = synth.from_ref(DIMS, src, 16, NCOL)
 
 
-def port_cpu_samples(nsamples: int, iters: int):
-    """Same samples with the numpy restatement (when oracle/_ref is absent)."""
-    from oracle import susy_np as O
-    from susy_b200 import synth
-    from susy_b200.rhmc_tables import rhmc
-    geo = O.Geometry(DIMS, -1)
-    prm = O.Params(lam=LAM, bmass=BMASS, G=G, N=NCOL)
-    U = synth.links(DIMS, NCOL, LINK_NOISE, LINK_SEED)
-    der = O.compute_derived(geo, prm, U)
-    src = synth.tf_source(DIMS, NCOL, SRC_SEED)
-    shifts = np.array(rhmc(NORDER, NROOT)["shift4"])
-    out = []
-    for _ in range(nsamples):
-        t0 = time.perf_counter()
-        _, it, _ = O.congrad_multi(geo, prm, U, der, src, shifts, iters, ERRORMIN)
-        out.append((time.perf_counter() - t0, it))
-    return out
+def _ref_sample(nshift, iters):
+    """Seconds per iteration of the CPU congrad_multi with nshift live
+    shifts (the first nshift poles), over `iters` iterations from the zero
+    initial guess (no shift freezes that early)."""
+    sh = _REF["shifts"][:nshift]
+    t0 = time.perf_counter()
+    if _REF["kind"] == "reference":
+        _, it, _ = _REF["ref"].congrad_multi(_REF["src"], sh, iters, ERRORMIN)
+    else:
+        from oracle import susy_np as O
+        geo, prm, U, der = _REF["port"]
+        _, it, _ = O.congrad_multi(geo, prm, U, der, _REF["src"], sh, iters, ERRORMIN)
+    return (time.perf_counter() - t0) / max(it, 1)
 
 
 def host_workers():
@@ -190,58 +224,138 @@ def host_workers():
     return max(1, min(n, 128))
 
 
-def _ref_worker(nsamples, iters, kind):
-    fn = reference_cpu_samples if kind == "reference" else port_cpu_samples
-    return fn(nsamples, iters)
+def solve_profile():
+    """(iterations, live shifts summed over the iterations) of the FP64
+    solve of this workload, from configs/solve_profile_12x12x12x24_u3.json
+    (configs/solve_profile.py)."""
+    with open(PROFILE_FILE) as f:
+        p = json.load(f)
+    return int(p["iterations"]), int(sum(p["live_shifts_per_iteration"])), p
 
 
-def cpu_samples(nsamples=1, iters=REF_SAMPLE_ITERS, workers=None):
-    """[(s/solve, ...)] and the cpu_baseline description.  The reference is
-    single threaded (its parallel path is MPI, which this image lacks), so
-    all host cores are used as independent single-core replicas, each
-    timing the same bounded sample; the value is the aggregate seconds per
-    solve of the host, time per replica / replicas."""
-    import multiprocessing as mp
-    from oracle.ref_ctypes import available
-    kind = "reference" if available(NCOL) else "port"
-    P = workers or host_workers()
-    ctx = mp.get_context("spawn")
-    with ctx.Pool(P) as pool:
-        res = pool.starmap(_ref_worker, [(nsamples, iters, kind)] * P)
-    per = [[dt / max(it, 1) * REF_ITERS for dt, it in r] for r in res]
-    vals = [statistics.mean(p[k] for p in per) / P for k in range(nsamples)]
-    per_iter = statistics.mean(r[-1][0] / max(r[-1][1], 1) for r in res)
-    desc = {"value": vals[-1], "unit": "s/solve", "cores": P, "kind": kind,
-            "sample": "%d of the %d iterations of the full solve, timed on each of %d "
-                      "single-core replicas of the reference running at once on the host "
-                      "(%.3f s/iteration each; the first iterations carry all 15 shifts), "
-                      "extrapolated to %d and divided by the replica count"
-                      % (res[-1][-1][1], REF_ITERS, P, per_iter, REF_ITERS)}
-    return vals, desc
+class CpuArm:
+    """The reference's CPU solve, sampled: the reference is single threaded
+    (its parallel path is MPI, which this image lacks), so every host core
+    runs an independent single-core replica and all of them time the same
+    bounded sample at once.  A sample is REF_SAMPLE_ITERS iterations of
+    congrad_multi with k live shifts; its per-iteration time is fitted as
+    t(k) = a + b k over the samples, and one solve costs
+    iterations * a + b * (live shifts summed over its iterations), the
+    schedule of the FP64 solve of this workload.  Seconds per solve of the
+    host = that / replicas."""
+
+    def __init__(self, workers=None):
+        import multiprocessing as mp
+        from oracle.ref_ctypes import available
+        self.kind = "reference" if available(NCOL) else "port"
+        self.P = workers or host_workers()
+        self.pool = mp.get_context("spawn").Pool(self.P, initializer=_ref_init,
+                                                 initargs=(self.kind,))
+        self.samples = []     # (k, seconds per iteration, averaged over replicas)
+
+    def sample(self, k):
+        t0 = time.perf_counter()
+        # bounded wait: a worker that died would otherwise leave the map
+        # waiting for good
+        per = self.pool.starmap_async(_ref_sample, [(k, REF_SAMPLE_ITERS)] * self.P,
+                                      chunksize=1).get(timeout=REF_SAMPLE_TIMEOUT)
+        self.samples.append((k, statistics.mean(per)))
+        return time.perf_counter() - t0
+
+    def close(self):
+        self.pool.terminate()
+
+    def value(self):
+        iters, live_sum, _ = solve_profile()
+        ks = np.array([k for k, _ in self.samples], dtype=float)
+        ts = np.array([t for _, t in self.samples])
+        if len(set(ks)) > 1:
+            b, a = np.polyfit(ks, ts, 1)
+        else:
+            b, a = ts.mean() / ks.mean(), 0.0
+        per_replica = iters * a + b * live_sum
+        desc = ("%d samples of %d iterations of the reference's congrad_multi with 1, 8 or "
+                "15 live shifts, on each of %d single-core replicas running at once on "
+                "the host; per-iteration time fitted as %.3f s + %.4f s per live shift and "
+                "summed over the FP64 solve's recorded schedule (%d iterations, %d "
+                "shift-iterations; configs/solve_profile_12x12x12x24_u3.json), divided "
+                "by the replica count"
+                % (len(self.samples), REF_SAMPLE_ITERS, self.P, a, b, iters, live_sum))
+        return per_replica / self.P, desc
 
 
-def cpu_baseline(iters=REF_SAMPLE_ITERS):
-    return cpu_samples(1, iters)[1]
+def cpu_baseline(nsamples=3):
+    arm = CpuArm()
+    try:
+        for i in range(nsamples):
+            arm.sample(REF_SAMPLE_SHIFTS[i % len(REF_SAMPLE_SHIFTS)])
+        v, desc = arm.value()
+    finally:
+        arm.close()
+    return {"value": v, "unit": "s/solve", "cores": arm.P, "kind": arm.kind, "sample": desc}
 
 
 # ---------------------------------------------------------------------------
 def run_reference_arm(args, rank, world):
     if rank != 0:
         return None
-    vals, base = cpu_samples(args.warmup + args.steps, REF_SAMPLE_ITERS)
-    v = statistics.mean(vals[args.warmup:])
+    arm = CpuArm()
+    walls = []
+    try:
+        for i in range(args.warmup + args.steps):
+            w = arm.sample(REF_SAMPLE_SHIFTS[i % len(REF_SAMPLE_SHIFTS)])
+            if i >= args.warmup:
+                walls.append(w)
+        arm.samples = arm.samples[args.warmup:]
+        v, desc = arm.value()
+    finally:
+        arm.close()
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "s/solve",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": v * 1e3, "higher_is_better": False, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "lattice": "12x12x12x24", "ncol": NCOL,
-                       "norder": NORDER, "nroot": NROOT, "parallelism": "replicas"},
-            "cpu_baseline": {"value": v, "unit": "s/solve", "cores": base["cores"],
-                             "kind": base["kind"], "sample": base["sample"]},
+            "ms_per_step": statistics.mean(walls) * 1e3,
+            "ms_per_step_note": "wall time of one bounded sample (all replicas); value is the "
+                                "full solve assembled from the samples",
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": bench_config({"solver": "reference congrad_multi (FP64, CPU)",
+                                    "parallelism": "replicas"}),
+            "cpu_baseline": {"value": v, "unit": "s/solve", "cores": arm.P, "kind": arm.kind,
+                             "sample": desc},
             "e2e": {"value": v, "unit": "s/solve", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return line
+
+
+def trajectories(lat, st, links, solvers):
+    """One RHMC trajectory per solver from the given links with the site and
+    node generators reseeded (TRAJ_SEED), timed with CUDA events on the
+    lattice's stream (the trajectory's host work included): 15 fermion x 3
+    gauge steps, trajectory length 1, Nroot 2, degree 15, error_per_site
+    1e-10, Metropolis.  The handle's links are left as they were."""
+    import torch
+    from susy_b200 import RHMC
+    runs = []
+    for name in solvers:
+        lat.set_links(links)
+        lat.seed(TRAJ_SEED)
+        r = RHMC(NORDER, NROOT, nstep=15, nstep_gauge=3, traj_length=1.0, niter=MAXCG,
+                 error_per_site=1e-10, solver=1 if name == "mixed" else 0)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        res = lat.update(r)
+        e1.record(st)
+        e1.synchronize()
+        runs.append({"solver": name, "s_per_traj": e0.elapsed_time(e1) / 1e3,
+                     "delta_S": res["delta_S"], "accept": bool(res["accept"]),
+                     "cg_iterations": res["iters"]})
+    lat.set_links(links)
+    by = {r["solver"]: r for r in runs}
+    out = {"nstep": 15, "nstep_gauge": 3, "traj_length": 1.0, "runs": runs}
+    if "mixed" in by and "fp64" in by:
+        out["delta_S_mixed_minus_fp64"] = by["mixed"]["delta_S"] - by["fp64"]["delta_S"]
+    return out
 
 
 def run_ours(args, rank, world, device):
@@ -256,8 +370,9 @@ def run_ours(args, rank, world, device):
     lat = Lattice(DIMS, NCOL, pbc=-1, lam=LAM, bmass=BMASS, G=G, device=device)
     st = torch.cuda.Stream(device=device)
     lat.set_stream(st.cuda_stream)
-    links = synth.links(DIMS, NCOL, LINK_NOISE, rank_seed(LINK_SEED, rank))
-    lat.set_links(synth.to_ref(DIMS, links))
+    links, links_info = workload_links()
+    lat.set_links(links)
+    # every replica solves its own source on the workload links
     src_host = synth.to_ref(DIMS, synth.tf_source(DIMS, NCOL, rank_seed(SRC_SEED, rank)))
     shifts = np.array(rhmc(NORDER, NROOT)["shift4"])
     src = lat.tf(64)
@@ -381,6 +496,13 @@ def run_ours(args, rank, world, device):
         h2d = host_src.nbytes
         d2h = sum(o.nbytes for o in outs)
 
+    # One full RHMC trajectory per solver (one GPU only: ~2 x 1-3 minutes),
+    # both from the workload links and the same random numbers, so both
+    # integrate the same trajectory and only the solves differ
+    traj = None
+    if world == 1 and not args.no_traj:
+        traj = trajectories(lat, st, links, ["mixed", "fp64"] if mixed else ["fp64", "mixed"])
+
     if rank != 0:
         return None
     value = seconds_per_solve(ms_max, args.steps, world)
@@ -389,9 +511,9 @@ def run_ours(args, rank, world, device):
             "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64" if not mixed else "f32+f64",
             "data": "synthetic",
-            "config": {"workload": WORKLOAD, "lattice": "12x12x12x24", "ncol": NCOL,
-                       "lambda": LAM, "bmass": BMASS, "G": G, "norder": NORDER,
-                       "nroot": NROOT, "solver": args.solver,
+            "config": bench_config({
+                       "links_checksums": links_info["checksums"],
+                       "solver": args.solver,
                        "parallelism": "replicas" if world > 1 else "single",
                        "l2": "working set ~3 GB > 126 MB L2; no flush",
                        "iterations_per_solve": iters[-1],
@@ -400,7 +522,7 @@ def run_ours(args, rank, world, device):
                            seconds_per_solve(other_ms, args.steps, world),
                        ("fp64" if mixed else "mixed") + "_iterations": other_iters,
                        "speedup_vs_fp64": (other_ms / ms_max) if mixed else 1.0,
-                       "fop_variant": lat.fop_variant(64)[0]},
+                       "fop_variant": lat.fop_variant(64)[0]}),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak,
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": traffic, "kernel": "fermion_op (FP64, in DSq)",
@@ -414,6 +536,11 @@ def run_ours(args, rank, world, device):
             "gpu_launches": launches,
             "e2e": {"value": seconds_per_solve(e2e_ms, args.steps, world) if e2e_ms else None,
                     "unit": "s/solve", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h}}
+    if traj:
+        line["trajectory"] = traj
+        t = {r["solver"]: r for r in traj["runs"]}
+        if "mixed" in t and "fp64" in t:
+            line["trajectory"]["speedup_vs_fp64"] = t["fp64"]["s_per_traj"] / t["mixed"]["s_per_traj"]
     if world == 1 and not args.no_cpu:
         try:
             line["cpu_baseline"] = cpu_baseline()
@@ -438,7 +565,10 @@ def run_dsq_case(args):
     lat = Lattice(dims, ncol, pbc=-1, lam=LAM, bmass=BMASS, G=G)
     st = torch.cuda.Stream()
     lat.set_stream(st.cuda_stream)
-    lat.set_links(synth.to_ref(dims, synth.links(dims, ncol, LINK_NOISE, LINK_SEED)))
+    if dims == DIMS and ncol == NCOL:
+        lat.set_links(workload_links()[0])
+    else:
+        lat.set_links(synth.to_ref(dims, synth.links(dims, ncol, LINK_NOISE, LINK_SEED)))
     src = synth.to_ref(dims, synth.tf_source(dims, ncol, SRC_SEED))
     peak, peak_kind = measured_peaks()
     variants = [args.variant] if args.variant >= 0 else list(range(FOP_NVARIANTS))
@@ -546,23 +676,20 @@ def run_traj_case(args):
     parameters of the metric's configuration (12^3x24 U(3), lambda 2,
     bmass 0.3, G 0.05, degree-15 rational approximation, Nroot 2, 15
     fermion steps x 3 gauge steps, error_per_site 1e-10, traj_length 1),
-    from the seeded near-identity links (not thermalised).  One warm-up
-    trajectory (mixed solver) moves the links off the start; then each
-    solver runs --steps trajectories from those same links and the same
-    random-number state (so every solver integrates the same trajectory and
-    only the solves differ), timed with CUDA events on the lattice's stream
-    (each trajectory's host work included).  Solvers: mixed (FP32
-    per-shift corrections), mixed with FP64 corrections, FP64."""
+    from the thermalised workload links.  Each solver runs --steps
+    trajectories from those links and the same random-number state (so
+    every solver integrates the same trajectory and only the solves differ),
+    timed with CUDA events on the lattice's stream (each trajectory's host
+    work included).  Solvers: mixed (FP32 per-shift corrections), mixed
+    with FP64 corrections, FP64."""
     import torch
-    from susy_b200 import Lattice, RHMC, synth
+    from susy_b200 import Lattice, RHMC
     lat = Lattice(DIMS, NCOL, pbc=-1, lam=LAM, bmass=BMASS, G=G)
     st = torch.cuda.Stream()
     lat.set_stream(st.cuda_stream)
-    lat.set_links(synth.to_ref(DIMS, synth.links(DIMS, NCOL, LINK_NOISE, LINK_SEED)))
+    start = workload_links()[0]
     mk = lambda solver: RHMC(NORDER, NROOT, nstep=15, nstep_gauge=3, traj_length=1.0,
                              niter=MAXCG, error_per_site=1e-10, solver=solver)
-    lat.update(mk(1))
-    start = lat.get_links()
     out = []
     for name, solver, c32 in (("mixed", 1, True), ("mixed_fp64_corrections", 1, False),
                               ("fp64", 0, True)):
@@ -599,6 +726,8 @@ def main():
     ap.add_argument("--solver", default="mixed", choices=["fp64", "mixed"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-traj", action="store_true",
+                    help="skip the per-solver trajectory timing of the one-GPU line")
     ap.add_argument("--dsq-case", action="store_true",
                     help="operator microbenchmark per kernel variant instead of the solve")
     ap.add_argument("--variant", type=int, default=-1)
@@ -611,7 +740,7 @@ def main():
     ap.add_argument("--traj-case", action="store_true",
                     help="full RHMC trajectories of the bench lattice, mixed and FP64 solver")
     ap.add_argument("--lattices", type=int, default=48)
-    ap.add_argument("--threads", type=int, default=16)
+    ap.add_argument("--threads", type=int, default=48)
     args = ap.parse_args()
     if args.dsq_case:
         run_dsq_case(args)

@@ -203,6 +203,12 @@ int susy_b200_mixed_params(susy_b200_lattice *h, double fp32_below, double relia
  * the FP64 true residual is checked after every pass) or in FP64 (fp32 = 0).
  * No counterpart in the reference.  fp32 not 0 or 1: SUSY_B200_EINVAL. */
 int susy_b200_mixed_correction(susy_b200_lattice *h, int fp32);
+/* Mixed solver, its FP32-operator phase: the residual ring, the shifted
+ * search vectors and the operator's input held in FP32 (fp32 = 1, the
+ * default; the solutions, the recurrences and every residual replacement
+ * stay FP64) or in FP64 (fp32 = 0).  No counterpart in the reference.
+ * fp32 < 0 only queries; returns the previous setting. */
+int susy_b200_mixed_vectors(susy_b200_lattice *h, int fp32);
 #define SUSY_B200_FOP_NVARIANTS 12   /* entries of ms_per_variant */
 int susy_b200_autotune(susy_b200_lattice *h);
 int susy_b200_fop_variant(susy_b200_lattice *h, int prec, int set_to, float *ms_per_variant);

@@ -176,12 +176,14 @@ class RefLattice:
         psim = np.zeros(len(shifts) * src.size)
         sr = C.c_double(0.0)
         tot = C.c_int(0)
-        self.lib.ref_congrad_multi.argtypes = [_dp, _dp, _dp, C.c_int, C.c_double,
+        self.lib.ref_congrad_multi.argtypes = [_dp, _dp, _dp, C.c_int, C.c_int, C.c_double,
                                                C.POINTER(C.c_double),
                                                C.POINTER(C.c_int)]
-        it = self.lib.ref_congrad_multi(_ptr(src), _ptr(psim), _ptr(shifts),
+        it = self.lib.ref_congrad_multi(_ptr(src), _ptr(psim), _ptr(shifts), len(shifts),
                                         int(MaxCG), float(errormin),
                                         C.byref(sr), C.byref(tot))
+        if it < 0:
+            raise ValueError("congrad_multi: %d shifts, the setup has fewer" % len(shifts))
         return psim.reshape(len(shifts), -1), it, sr.value
 
     def fermion_force(self, eps, src, sol):

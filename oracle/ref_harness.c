@@ -208,16 +208,24 @@ void ref_DSq(double *src, double *dest) {
 }
 
 /* congrad_multi with caller-chosen shifts; psim is Norder contiguous fields */
-int ref_congrad_multi(double *src, double *psim, double *shifts, int MaxCG,
+/* congrad_multi on nshift shifts (1 <= nshift <= the setup's Norder): the
+ * reference loops over the global Norder, so it is set to nshift for the
+ * call and restored after it */
+int ref_congrad_multi(double *src, double *psim, double *shifts, int nshift, int MaxCG,
                       double errormin, double *size_r, int *total) {
-  int j, it;
+  int j, it, norder_setup = Norder;
   Real sr = 0.0;
-  Twist_Fermion **ps = malloc(sizeof(Twist_Fermion *) * Norder);
-  for (j = 0; j < Norder; j++) {
+  Twist_Fermion **ps;
+  if (nshift < 1 || nshift > norder_setup)
+    return -1;
+  ps = malloc(sizeof(Twist_Fermion *) * nshift);
+  for (j = 0; j < nshift; j++) {
     ps[j] = (Twist_Fermion *)(psim + (size_t)j * sites_on_node * TF_DOUBLES);
     shift[j] = shifts[j];
   }
+  Norder = nshift;
   it = congrad_multi((Twist_Fermion *)src, ps, MaxCG, errormin, &sr);
+  Norder = norder_setup;
   *size_r = sr;
   if (total)
     *total = total_iters;

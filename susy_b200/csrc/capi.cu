@@ -252,6 +252,7 @@ susy_b200_lattice* solver_shadow(susy_b200_lattice* h) {
   c->mix_switch = h->mix_switch;
   c->mix_reliable = h->mix_reliable;
   c->mix_correct32 = h->mix_correct32;
+  c->mix_vec32 = h->mix_vec32;
   for (int pi = 0; pi < 2; pi++) {
     c->fop_variant[pi] = h->fop_variant[pi];
     for (int v = 0; v < SUSY_B200_FOP_NVARIANTS; v++) c->fop_ms[pi][v] = h->fop_ms[pi][v];
@@ -343,7 +344,7 @@ void susy_b200_destroy(susy_b200_lattice* h) {
   }
   for (int i = 0; i < SUSY_NPART; i++)
     if (h->part[i]) cudaFree(h->part[i]);
-  for (std::vector<void*>* v : {&h->extra, &h->sols, &h->pvec64, &h->pvec32, &h->ring, &h->gsrc,
+  for (std::vector<void*>* v : {&h->extra, &h->sols, &h->pvec64, &h->pvec32, &h->ring, &h->vec32, &h->gsrc,
                                 &h->gr_psim, &h->traj_psim, &h->extra5, &h->refine})
     for (void* p : *v)
       if (p) cudaFree(p);
@@ -384,6 +385,16 @@ int susy_b200_mixed_correction(susy_b200_lattice* h, int fp32) {
   if (!h || (fp32 != 0 && fp32 != 1)) return SUSY_B200_EINVAL;
   h->mix_correct32 = fp32;
   return SUSY_B200_OK;
+}
+
+int susy_b200_mixed_vectors(susy_b200_lattice* h, int fp32) {
+  if (!h || fp32 > 1) return SUSY_B200_EINVAL;
+  const int prev = h->mix_vec32;
+  if (fp32 >= 0) {
+    h->mix_vec32 = fp32;
+    if (h->shadow) h->shadow->mix_vec32 = fp32;
+  }
+  return prev;
 }
 
 int susy_b200_dev_congrad_multi_learned(susy_b200_lattice* h, susy_b200_net* net,

@@ -435,7 +435,24 @@ void ms_update_p0(MsState* st, const MsVecs& v, int prec, long n, cudaStream_t s
 // dependent single-block launch per iteration; it resets the counter for
 // the next launch.  Every block reads skip before the last one can change
 // it.
-template <typename MT>
+// RT: type of the ring (FP64, or FP32 with f32 vectors)
+template <typename VT> SUSY_D double2 ld2(const VT* p, long i) {
+  const VT v = p[i];
+  return make_double2(v.x, v.y);
+}
+template <typename VT> SUSY_D void st2(VT* p, long i, double2 v);
+template <> SUSY_D void st2<double2>(double2* p, long i, double2 v) { p[i] = v; }
+template <> SUSY_D void st2<float2>(float2* p, long i, double2 v) {
+  p[i] = make_float2((float)v.x, (float)v.y);
+}
+// v as a VT holds it
+template <typename VT> SUSY_D double2 rnd2(double2 v);
+template <> SUSY_D double2 rnd2<double2>(double2 v) { return v; }
+template <> SUSY_D double2 rnd2<float2>(double2 v) {
+  return make_double2((double)(float)v.x, (double)(float)v.y);
+}
+
+template <typename MT, typename RT>
 __global__ void __launch_bounds__(UT) k_msb_update_r(MsState* st, MsBlockVecs v, long n,
                                                      double* part) {
   static_assert(UT == ST, "the last block runs the ST-thread scalar step");
@@ -444,18 +461,19 @@ __global__ void __launch_bounds__(UT) k_msb_update_r(MsState* st, MsBlockVecs v,
   if (st->skip) return;
   const int it = st->iter;
   const double b0 = st->beta_i[0];
-  const double2* rin = (const double2*)v.ring[(it - 1) % (MS_BLK + 1)];
-  double2* rout = (double2*)v.ring[it % (MS_BLK + 1)];
+  const RT* rin = (const RT*)v.ring[(it - 1) % (MS_BLK + 1)];
+  RT* rout = (RT*)v.ring[it % (MS_BLK + 1)];
   const MT* mp = (const MT*)(sizeof(MT) == 16 ? v.mp : v.mp32);
   double acc = 0.0;
   // grid-stride: few blocks, so the scalar kernel sums few partials
   for (long i = (long)blockIdx.x * UT + threadIdx.x; i < n; i += (long)gridDim.x * UT) {
-    double2 r = rin[i];
+    double2 r = ld2(rin, i);
     const MT m = mp[i];
     r.x += b0 * m.x;
     r.y += b0 * m.y;
-    rout[i] = r;
-    acc += r.x * r.x + r.y * r.y;
+    st2(rout, i, r);
+    const double2 rr = rnd2<RT>(r);   // |r|^2 of the residual as stored
+    acc += rr.x * rr.x + rr.y * rr.y;
   }
   acc = block_sum<UT>(acc);
   if (threadIdx.x == 0) {
@@ -470,17 +488,17 @@ __global__ void __launch_bounds__(UT) k_msb_update_r(MsState* st, MsBlockVecs v,
 }
 
 // p0 = r(i) + alpha_0 p0 (and its FP32 copy for an FP32 operator)
+template <typename RT>
 __global__ void __launch_bounds__(UT) k_msb_update_p0(MsState* st, MsBlockVecs v, long n) {
   if (st->skip_b) return;
   const long i = (long)blockIdx.x * UT + threadIdx.x;
   if (i >= n) return;
   const double a0 = st->alpha[0];
-  const double2 r = ((const double2*)v.ring[st->iter % (MS_BLK + 1)])[i];
-  double2* pp = (double2*)v.p0 + i;
-  double2 p = *pp;
+  const double2 r = ld2((const RT*)v.ring[st->iter % (MS_BLK + 1)], i);
+  double2 p = ld2((const RT*)v.p0, i);
   p.x = r.x + a0 * p.x;
   p.y = r.y + a0 * p.y;
-  *pp = p;
+  st2((RT*)v.p0, i, p);
   if (v.p0_32) ((float2*)v.p0_32)[i] = make_float2((float)p.x, (float)p.y);
 }
 
@@ -488,6 +506,7 @@ __global__ void __launch_bounds__(UT) k_msb_update_p0(MsState* st, MsBlockVecs v
 // true residual rt, and the search vectors built from the old r(k) get the
 // same correction d = rt - r(k) so that p0 = r(k) + alpha p0_prev and
 // P_j = zeta_j r(k) + alpha_j P_j,prev keep holding (zeta_0 = 1)
+template <typename RT>
 __global__ void __launch_bounds__(UT) k_msb_replace(MsState* st, MsBlockVecs v, long n,
                                                     const double2* rt) {
   __shared__ double z[MS_MAXS];
@@ -501,24 +520,23 @@ __global__ void __launch_bounds__(UT) k_msb_replace(MsState* st, MsBlockVecs v, 
   __syncthreads();
   const long i = (long)blockIdx.x * UT + threadIdx.x;
   if (i >= n) return;
-  double2* r = (double2*)v.ring[st->iter % (MS_BLK + 1)] + i;
+  RT* r = (RT*)v.ring[st->iter % (MS_BLK + 1)];
   const double2 t = rt[i];
-  const double2 d = make_double2(t.x - r->x, t.y - r->y);
-  *r = t;
-  double2* p0 = (double2*)v.p0 + i;
-  double2 p = *p0;
+  const double2 r0 = ld2(r, i);
+  const double2 d = make_double2(t.x - r0.x, t.y - r0.y);
+  st2(r, i, t);
+  double2 p = ld2((const RT*)v.p0, i);
   p.x += d.x;
   p.y += d.y;
-  *p0 = p;
+  st2((RT*)v.p0, i, p);
   if (v.p0_32) ((float2*)v.p0_32)[i] = make_float2((float)p.x, (float)p.y);
 #pragma unroll 1
   for (int j = 0; j < ns; j++) {
     if (!lv[j]) continue;
-    double2* pj = (double2*)v.P[j] + i;
-    double2 q = *pj;
+    double2 q = ld2((const RT*)v.P[j], i);
     q.x += z[j] * d.x;
     q.y += z[j] * d.y;
-    *pj = q;
+    st2((RT*)v.P[j], i, q);
   }
 }
 
@@ -541,6 +559,7 @@ __global__ void k_msb_set_rsq(MsState* st, double rsq) {
 // The block pass: every live shift's psi_j and P_j advanced over the
 // recorded iterations.  Each CTA first derives the combination
 // coefficients of every live shift in shared memory.
+template <typename RT>
 __global__ void __launch_bounds__(UT) k_msb_block(MsState* st, MsBlockVecs v, long n) {
   __shared__ double cx0[MS_MAXS], cp0[MS_MAXS];
   __shared__ double cxr[MS_MAXS][MS_BLK], cpr[MS_MAXS][MS_BLK];
@@ -586,13 +605,12 @@ __global__ void __launch_bounds__(UT) k_msb_block(MsState* st, MsBlockVecs v, lo
   double2 R[MS_BLK];
 #pragma unroll
   for (int q = 0; q < MS_BLK; q++)
-    R[q] = q < L ? ((const double2*)v.ring[(k + 1 + q) % (MS_BLK + 1)])[i] : make_double2(0, 0);
+    R[q] = q < L ? ld2((const RT*)v.ring[(k + 1 + q) % (MS_BLK + 1)], i) : make_double2(0, 0);
 #pragma unroll 1
   for (int j = 0; j < ns; j++) {
     if (!lv[j]) continue;
-    double2* pp = (double2*)v.P[j] + i;
     double2* xp = (double2*)v.x[j] + i;
-    const double2 p = *pp;
+    const double2 p = ld2((const RT*)v.P[j], i);
     double2 x = *xp;
     double2 pn;
     x.x -= cx0[j] * p.x;
@@ -607,7 +625,7 @@ __global__ void __launch_bounds__(UT) k_msb_block(MsState* st, MsBlockVecs v, lo
       pn.y += cpr[j][q] * R[q].y;
     }
     *xp = x;
-    *pp = pn;
+    st2((RT*)v.P[j], i, pn);
   }
 }
 
@@ -627,10 +645,12 @@ __global__ void k_msb_block_reset(MsState* st) {
 void msb_update_r(MsState* st, const MsBlockVecs& v, long n, double* part, bool mp32,
                   cudaStream_t s) {
   const int nb = vec_blocks(n) < 1184 ? vec_blocks(n) : 1184;
-  if (mp32)
-    count_launch(), k_msb_update_r<float2><<<nb, UT, 0, s>>>(st, v, n, part);
+  if (v.f32)
+    count_launch(), k_msb_update_r<float2, float2><<<nb, UT, 0, s>>>(st, v, n, part);
+  else if (mp32)
+    count_launch(), k_msb_update_r<float2, double2><<<nb, UT, 0, s>>>(st, v, n, part);
   else
-    count_launch(), k_msb_update_r<double2><<<nb, UT, 0, s>>>(st, v, n, part);
+    count_launch(), k_msb_update_r<double2, double2><<<nb, UT, 0, s>>>(st, v, n, part);
 }
 
 // Residual replacement: r(k) <- rt with the matching search-vector
@@ -638,16 +658,25 @@ void msb_update_r(MsState* st, const MsBlockVecs& v, long n, double* part, bool 
 // follows it)
 void msb_replace(MsState* st, const MsBlockVecs& v, long n, const void* rt, double rsq,
                  cudaStream_t s) {
-  count_launch(), k_msb_replace<<<vec_blocks(n), UT, 0, s>>>(st, v, n, (const double2*)rt);
+  if (v.f32)
+    count_launch(), k_msb_replace<float2><<<vec_blocks(n), UT, 0, s>>>(st, v, n, (const double2*)rt);
+  else
+    count_launch(), k_msb_replace<double2><<<vec_blocks(n), UT, 0, s>>>(st, v, n, (const double2*)rt);
   count_launch(), k_msb_set_rsq<<<1, 1, 0, s>>>(st, rsq);
 }
 
 void msb_update_p0(MsState* st, const MsBlockVecs& v, long n, cudaStream_t s) {
-  count_launch(), k_msb_update_p0<<<vec_blocks(n), UT, 0, s>>>(st, v, n);
+  if (v.f32)
+    count_launch(), k_msb_update_p0<float2><<<vec_blocks(n), UT, 0, s>>>(st, v, n);
+  else
+    count_launch(), k_msb_update_p0<double2><<<vec_blocks(n), UT, 0, s>>>(st, v, n);
 }
 
 void msb_block(MsState* st, const MsBlockVecs& v, long n, cudaStream_t s) {
-  count_launch(), k_msb_block<<<vec_blocks(n), UT, 0, s>>>(st, v, n);
+  if (v.f32)
+    count_launch(), k_msb_block<float2><<<vec_blocks(n), UT, 0, s>>>(st, v, n);
+  else
+    count_launch(), k_msb_block<double2><<<vec_blocks(n), UT, 0, s>>>(st, v, n);
   count_launch(), k_msb_block_reset<<<1, MS_MAXS, 0, s>>>(st);
 }
 

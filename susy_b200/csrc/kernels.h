@@ -56,6 +56,8 @@ struct MsVecs {
 // (P[0] a copy of the operator input p0 at that point); x[j] the solutions.
 // p0_32 / mp32: FP32 operator input and output when the operator runs in
 // FP32 (p0_32 written by the p0 update; nullptr in FP64).
+// f32 = 1: ring, P and p0 are FP32 fields (the operator's input is p0
+// itself, its output mp32); the solutions x stay FP64.
 struct MsBlockVecs {
   void* ring[MS_BLK + 1];
   void* P[MS_MAXS];
@@ -64,6 +66,7 @@ struct MsBlockVecs {
   void* mp;
   void* p0_32;
   void* mp32;
+  int f32;
 };
 
 // fermion_op.cu, fermion_op_rows.cu

@@ -36,6 +36,8 @@ struct susy_b200_lattice {
   std::vector<void*> pvec64;  // p_j of the FP64 multi-shift CG
   std::vector<void*> pvec32;
   std::vector<void*> ring;    // residual ring of the blocked FP64 solver
+  std::vector<void*> vec32;   // FP32 ring and search vectors of the mixed solver's FP32 phase
+  int mix_vec32 = 1;          // mixed solver: FP32 vectors in its FP32 phase
   double* meas = nullptr;     // measurement partials
   size_t meas_n = 0;
   int ms_blocked = 1;         // FP64 multi-shift CG: blocked vector update

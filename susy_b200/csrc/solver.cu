@@ -116,6 +116,13 @@ static void* ring_field(susy_b200_lattice* h, int q) {
   return h->ring[q];
 }
 
+// FP32 fields of the mixed solver's FP32 phase: residual ring slots
+// 0..MS_BLK, then the search vectors P_j at MS_BLK + 1 + j
+static void* vec32_field(susy_b200_lattice* h, int q) {
+  while ((int)h->vec32.size() <= q) h->vec32.push_back(dalloc(h, field_bytes(h, NTF, 32)));
+  return h->vec32[q];
+}
+
 // One captured chunk of solver iterations.  Capture is thread-local, so
 // other host threads driving other lattices (susy_b200_update_batch) may
 // keep launching meanwhile.  If capture or instantiation fails the chunk
@@ -170,8 +177,10 @@ static double true_residual(susy_b200_lattice* h, const void* b, const void* x, 
 //
 // mixed = false: FP64 throughout (the reference's solver).
 // mixed = true: the operator runs in FP64 until |r| < mix_switch |src|
-// (handle setting, default 3e-5) and in FP32 after that; every vector,
-// the recurrences and the solutions stay FP64.  Once the operator is FP32,
+// (handle setting, default 3e-5) and in FP32 after that; with mix_vec32
+// (the default) the residual ring, the search vectors and the operator's
+// input are FP32 fields from then on too (half the vector traffic of the
+// FP32 phase), while the recurrences and the solutions stay FP64.  Once the operator is FP32,
 // the iterated residual drifts from the true one by the FP32 rounding of
 // each product, so at block boundaries, whenever |r| fell by mix_reliable
 // (default 1e-2) since the last check and when the solve stops, the FP64
@@ -219,6 +228,7 @@ static int ms_run_block(susy_b200_lattice* h, const void* src, void* const* psim
   v.mp = mp;
   v.p0_32 = nullptr;
   v.mp32 = mp32;
+  v.f32 = 0;
   // r(0) = src, p0 = P_j = src, psi_j = 0   (congrad_multi.c:47-57)
   cudaMemcpyAsync(v.ring[0], src, bv, cudaMemcpyDeviceToDevice, s);
   cudaMemcpyAsync(p0, src, bv, cudaMemcpyDeviceToDevice, s);
@@ -304,11 +314,31 @@ static int ms_run_block(susy_b200_lattice* h, const void* src, void* const* psim
       const double rsq = *pd;
       const int it = pw[1];
       if (!fp32_op && !stop && rsq < h->mix_switch * h->mix_switch * bnorm) {
-        // the operator input from now on: an FP32 copy of p0, kept by the
-        // p0 update
         fp32_op = true;
-        v.p0_32 = p0_32;
         convert_field(n, p0, 64, p0_32, 32, s);
+        if (h->mix_vec32) {
+          // FP32 vectors from here on (this poll follows a block pass, so
+          // the search vectors are current and the residual of this
+          // iteration is the only ring slot the next steps read): the
+          // operator's input is the FP32 p0 itself; the solutions stay FP64
+          const int slot = pw[1] % (MS_BLK + 1);
+          for (int q = 0; q <= MS_BLK; q++)
+            if (!vec32_field(h, q)) return set_err(h, SUSY_B200_ENOMEM);
+          convert_field(n, v.ring[slot], 64, vec32_field(h, slot), 32, s);
+          for (int q = 0; q <= MS_BLK; q++) v.ring[q] = vec32_field(h, q);
+          for (int j = 0; j < norder; j++) {
+            void* p32 = vec32_field(h, MS_BLK + 1 + j);
+            if (!p32) return set_err(h, SUSY_B200_ENOMEM);
+            convert_field(n, v.P[j], 64, p32, 32, s);
+            v.P[j] = p32;
+          }
+          v.p0 = p0_32;
+          v.f32 = 1;
+        } else {
+          // the operator input from now on: an FP32 copy of p0, kept by the
+          // p0 update
+          v.p0_32 = p0_32;
+        }
       } else if (fp32_op && (stop || rsq < h->mix_reliable * h->mix_reliable * last_true)) {
         // reliable update at the block boundary: psi_0 is current
         void* rt64 = refine_field(h, 4, 64);

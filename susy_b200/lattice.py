@@ -166,6 +166,8 @@ def load_library(path: str = LIB_PATH):
     L.susy_b200_pf_streams.argtypes = [_vp, C.c_int]
     L.susy_b200_cg_blocked.restype = C.c_int
     L.susy_b200_cg_blocked.argtypes = [_vp, C.c_int]
+    L.susy_b200_mixed_vectors.restype = C.c_int
+    L.susy_b200_mixed_vectors.argtypes = [_vp, C.c_int]
     L.susy_b200_cg_freeze_iterations.restype = C.c_int
     L.susy_b200_cg_freeze_iterations.argtypes = [_vp, C.POINTER(C.c_int), C.c_int]
     L.susy_b200_dev_congrad_multi.argtypes = [_vp, _vp, C.POINTER(_vp), C.c_int, _dp, C.c_int,
@@ -443,6 +445,11 @@ class Lattice:
         """Mixed solver: per-shift correction solves with the FP32 operator
         (iterative refinement against the FP64 true residual) or in FP64."""
         self._check(self.lib.susy_b200_mixed_correction(self.h, 1 if fp32 else 0))
+
+    def mixed_vectors(self, fp32: int = -1) -> int:
+        """Mixed solver: FP32 (1) or FP64 (0) ring and search vectors in its
+        FP32-operator phase; returns the previous setting."""
+        return self._check(self.lib.susy_b200_mixed_vectors(self.h, int(fp32)))
 
     def measure(self) -> dict:
         """Measurements of control.c:85-138 on the current links, keyed as

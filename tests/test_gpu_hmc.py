@@ -199,10 +199,14 @@ def test_mixed_and_fp64_integrate_the_same_trajectory(N):
     assert abs(out["mixed"][0]["delta_S"] - out["fp64"][0]["delta_S"]) < 1e-7
 
 
+@pytest.mark.parametrize("vec32", [1, 0])
 @pytest.mark.parametrize("N", [2, 3])
-def test_mixed_solver_reaches_fp64_residual(N):
+def test_mixed_solver_reaches_fp64_residual(N, vec32):
+    """Every shift's FP64 true residual within the bound, with FP32 (vec32 =
+    1, the default) or FP64 ring and search vectors in the FP32 phase."""
     dims = (4, 4, 4, 8)
     lat, geo, prm, U = make(dims, N, G=0.05)
+    lat.mixed_vectors(vec32)
     der = O.compute_derived(geo, prm, U)
     src = synth.tf_source(dims, N, 31)
     shifts = np.array(rhmc_table(15, 1)["shift4"])
