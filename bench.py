@@ -15,7 +15,7 @@ starts; the working set (~3 GB) is larger than L2, so no flush is needed.
                   [--solver mixed|fp64] [--no-traj]
 
 The timed solver is the mixed one by default (FP64 operator until
-|r| < 3e-5 |src|, FP32 operator after, FP64 residual replacement and
+|r| < 3e-4 |src|, FP32 operator after, FP64 residual replacement and
 per-shift FP64 check: the same FP64 true-residual bound as the FP64 solver,
 reported as true_residual_rel_max); the FP64 solver of the reference's
 recurrences is timed right after it in the same run (fp64_s_per_solve).

@@ -192,7 +192,7 @@ int susy_b200_pf_streams(susy_b200_lattice *h, int on);
  * Returns the previous setting. */
 int susy_b200_set_solver(susy_b200_lattice *h, int solver);
 /* Mixed-precision solver settings (no reference counterpart): the operator
- * runs in FP32 once |r| < fp32_below |src| (default 3e-5); with the FP32
+ * runs in FP32 once |r| < fp32_below |src| (default 3e-4); with the FP32
  * operator the FP64 true residual replaces the iterated one whenever |r|
  * fell by reliable_factor (default 1e-2) since the last replacement.
  * 0 < fp32_below <= 1, 0 < reliable_factor < 1, else SUSY_B200_EINVAL. */
@@ -203,10 +203,20 @@ int susy_b200_mixed_params(susy_b200_lattice *h, double fp32_below, double relia
  * the FP64 true residual is checked after every pass) or in FP64 (fp32 = 0).
  * No counterpart in the reference.  fp32 not 0 or 1: SUSY_B200_EINVAL. */
 int susy_b200_mixed_correction(susy_b200_lattice *h, int fp32);
-/* Mixed solver, its FP32-operator phase: the residual ring, the shifted
- * search vectors and the operator's input held in FP32 (fp32 = 1, the
- * default; the solutions, the recurrences and every residual replacement
- * stay FP64) or in FP64 (fp32 = 0).  No counterpart in the reference.
+/* The reference's compile-time RESCALE option (susy/defines.h:30; its
+ * susy_cheb and susy_mode targets define it): fermion_op doubles the site
+ * component of its input and of its output (utilities.c:795-797,841-844),
+ * for every operator application of the handle (fermion_op, DSq and the
+ * solvers; the fermion force, which the reference marks "not yet
+ * conserving" under RESCALE, update_h.c:697-702, is unchanged).  on = 1
+ * sets it, 0 clears it, < 0 only queries; returns the previous setting. */
+int susy_b200_set_rescale(susy_b200_lattice *h, int on);
+/* Mixed solver, its FP32-operator phase: the residual ring and the
+ * operator's input held in FP32 (fp32 = 1; the shifted search vectors, the
+ * solutions, the recurrences and every residual replacement stay FP64) or
+ * in FP64 (fp32 = 0, the default: on the 12^3x24 U(3) benchmark the FP32
+ * residuals cost more correction iterations than they save).  No
+ * counterpart in the reference.
  * fp32 < 0 only queries; returns the previous setting. */
 int susy_b200_mixed_vectors(susy_b200_lattice *h, int fp32);
 #define SUSY_B200_FOP_NVARIANTS 12   /* entries of ms_per_variant */

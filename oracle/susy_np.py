@@ -268,6 +268,10 @@ class Params:
     kappa_u1: float = 0.0
     G: float = 0.0
     N: int = 2
+    # the reference's compile-time RESCALE (defines.h:30; set for its
+    # susy_cheb and susy_mode programs): fermion_op doubles the site
+    # component of its input and of its output (utilities.c:795,841)
+    rescale: bool = False
 
     @property
     def kappa(self):
@@ -339,6 +343,9 @@ def fermion_op(geo: Geometry, prm: Params, U, der: Derived, src, sign: int):
         raise ValueError("incorrect sign in fermion_op: %d" % sign)
     N = U.shape[-1]
     s = src if sign == 1 else adj(src)
+    if prm.rescale:                              # utilities.c:795-797
+        s = s.copy()
+        s[0] = 2.0 * s[0]
     eta = s[0]
     psi = s[1:6]
     V = geo.V
@@ -414,6 +421,8 @@ def fermion_op(geo: Geometry, prm: Params, U, der: Derived, src, sign: int):
             bcol(geo.bc(a, b, c)) * (geo.shift(chi, a, b, c) @ adj(geo.shift(U[c], a, b)))
             - bcol(geo.bc(a, b))
             * (adj(geo.shift(U[c], c, sign=-1)) @ geo.shift(chi, a, b)))
+    if prm.rescale:                              # utilities.c:841-844
+        dest[0] = 2.0 * dest[0]
     if sign == 1:
         return dest
     return -adj(dest)

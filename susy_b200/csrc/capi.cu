@@ -122,13 +122,18 @@ void refresh_low(susy_b200_lattice* h) {
   convert_field(25L * h->g.S, h->pd, 64, h->pd32, 32, h->stream);
 }
 
+// With the RESCALE option only the table-driven kernels (variants from
+// FOP_COMPACT on) apply the factor; a variant below them is replaced by
+// FOP_SITE_MAJOR_OCC.
 static int launch_variant(susy_b200_lattice* h, const void* src, void* dst, int sign, int prec,
                           const void* add, double addc, double* dot, const int* skip, int v) {
+  const double es = h->rescale ? 2.0 : 1.0;
+  if (h->rescale && v < FOP_COMPACT) v = FOP_SITE_MAJOR_OCC;
   if (prec == 64)
     return fermion_op<double>(h->g, h->N, h->U, h->Uinv, h->pd, src, dst, sign, h->G, add, addc,
-                              dot, skip, v, h->nbrtab, h->stream);
+                              dot, skip, v, h->nbrtab, h->stream, es);
   return fermion_op<float>(h->g, h->N, h->U32, h->Uinv32, h->pd32, src, dst, sign, h->G, add,
-                           addc, dot, skip, v, h->nbrtab, h->stream);
+                           addc, dot, skip, v, h->nbrtab, h->stream, es);
 }
 
 // Project-written autotuner: time one D^dag D with every kernel variant on
@@ -145,8 +150,8 @@ int autotune_fop(susy_b200_lattice* h, int prec) {
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
   float best = 1e30f;
-  int bestv = FOP_MAT;
-  for (int v = 0; v < FOP_NVARIANTS; v++) {
+  int bestv = h->rescale ? FOP_SITE_MAJOR_OCC : FOP_MAT;
+  for (int v = h->rescale ? FOP_COMPACT : 0; v < FOP_NVARIANTS; v++) {
     launch_variant(h, a, b, 1, prec, nullptr, 0.0, nullptr, nullptr, v);
     cudaEventRecord(e0, h->stream);
     for (int r = 0; r < 3; r++) {
@@ -253,6 +258,7 @@ susy_b200_lattice* solver_shadow(susy_b200_lattice* h) {
   c->mix_reliable = h->mix_reliable;
   c->mix_correct32 = h->mix_correct32;
   c->mix_vec32 = h->mix_vec32;
+  c->rescale = h->rescale;
   for (int pi = 0; pi < 2; pi++) {
     c->fop_variant[pi] = h->fop_variant[pi];
     for (int v = 0; v < SUSY_B200_FOP_NVARIANTS; v++) c->fop_ms[pi][v] = h->fop_ms[pi][v];
@@ -385,6 +391,16 @@ int susy_b200_mixed_correction(susy_b200_lattice* h, int fp32) {
   if (!h || (fp32 != 0 && fp32 != 1)) return SUSY_B200_EINVAL;
   h->mix_correct32 = fp32;
   return SUSY_B200_OK;
+}
+
+int susy_b200_set_rescale(susy_b200_lattice* h, int on) {
+  if (!h || on > 1) return SUSY_B200_EINVAL;
+  const int prev = h->rescale;
+  if (on >= 0) {
+    h->rescale = on;
+    if (h->shadow) h->shadow->rescale = on;
+  }
+  return prev;
 }
 
 int susy_b200_mixed_vectors(susy_b200_lattice* h, int fp32) {

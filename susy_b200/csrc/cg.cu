@@ -533,10 +533,11 @@ __global__ void __launch_bounds__(UT) k_msb_replace(MsState* st, MsBlockVecs v, 
 #pragma unroll 1
   for (int j = 0; j < ns; j++) {
     if (!lv[j]) continue;
-    double2 q = ld2((const RT*)v.P[j], i);
+    double2* pj = (double2*)v.P[j] + i;
+    double2 q = *pj;
     q.x += z[j] * d.x;
     q.y += z[j] * d.y;
-    st2((RT*)v.P[j], i, q);
+    *pj = q;
   }
 }
 
@@ -610,7 +611,8 @@ __global__ void __launch_bounds__(UT) k_msb_block(MsState* st, MsBlockVecs v, lo
   for (int j = 0; j < ns; j++) {
     if (!lv[j]) continue;
     double2* xp = (double2*)v.x[j] + i;
-    const double2 p = ld2((const RT*)v.P[j], i);
+    double2* pp = (double2*)v.P[j] + i;
+    const double2 p = *pp;
     double2 x = *xp;
     double2 pn;
     x.x -= cx0[j] * p.x;
@@ -625,7 +627,7 @@ __global__ void __launch_bounds__(UT) k_msb_block(MsState* st, MsBlockVecs v, lo
       pn.y += cpr[j][q] * R[q].y;
     }
     *xp = x;
-    st2((RT*)v.P[j], i, pn);
+    *pp = pn;
   }
 }
 

@@ -130,7 +130,8 @@ SUSY_D void run_pattern(Mat<N, R>& acc, const FopArgs<R>& a, int s, unsigned bcm
         Ln = ldm<N, R, AL>(fl, Tn.kl, a.nbrtab[(size_t)Tn.dl * S + s], S);
         Rn = ldm<N, R, AR>(fr, Tn.kr, a.nbrtab[(size_t)Tn.dr * S + s], S);
       }
-      mac<0>(acc, (R)T.coef * bc_of<R>(bcm, T.bcdt, pbc), L, Rm);
+      mac<0>(acc, (R)T.coef * bc_of<R>(bcm, T.bcdt, pbc) * ((LF ? T.kl : T.kr) ? (R)1 : a.eta_scale),
+             L, Rm);
       L = Ln;
       Rm = Rn;
       T = Tn;
@@ -141,7 +142,8 @@ SUSY_D void run_pattern(Mat<N, R>& acc, const FopArgs<R>& a, int s, unsigned bcm
       const FTerm T = c_terms[t];
       Mat<N, R> L = ldm<N, R, AL>(fl, T.kl, a.nbrtab[(size_t)T.dl * S + s], S);
       Mat<N, R> Rm = ldm<N, R, AR>(fr, T.kr, a.nbrtab[(size_t)T.dr * S + s], S);
-      mac<0>(acc, (R)T.coef * bc_of<R>(bcm, T.bcdt, pbc), L, Rm);
+      mac<0>(acc, (R)T.coef * bc_of<R>(bcm, T.bcdt, pbc) * ((LF ? T.kl : T.kr) ? (R)1 : a.eta_scale),
+             L, Rm);
     }
   }
 }
@@ -174,6 +176,7 @@ fermion_op_compact_kernel(FopArgs<R> a) {
       else if (comp <= NUMLINK)
         det_stol_rt<N, R, SIGN>(acc, a, c, comp - 1);
     }
+    if (comp == 0) eta_rescale(acc, a.eta_scale);
     if (SIGN < 0) {
       Mat<N, R> t = acc;
 #pragma unroll
@@ -233,7 +236,7 @@ SUSY_D void run_pattern_pp(ACC& acc, const FopArgs<R>& a, int s, unsigned bcm, i
       const int ir = shn ? shn[T.sr * CT_THREADS + threadIdx.x] : a.nbrtab[(size_t)T.dr * S + s];
       const Mat<N, R> L = ldm<N, R, AL>(fl, T.kl, il, S);
       const Mat<N, R> Rm = ldm<N, R, AR>(fr, T.kr, ir, S);
-      acc.add((R)T.coef * bc_of<R>(bcm, T.bcdt, pbc), L, Rm);
+      acc.add((R)T.coef * bc_of<R>(bcm, T.bcdt, pbc) * ((LF ? T.kl : T.kr) ? (R)1 : a.eta_scale), L, Rm);
     }
     return;
   }
@@ -250,7 +253,8 @@ SUSY_D void run_pattern_pp(ACC& acc, const FopArgs<R>& a, int s, unsigned bcm, i
       LB = ldm<N, R, AL>(fl, TB.kl, a.nbrtab[(size_t)TB.dl * S + s], S);
       RB = ldm<N, R, AR>(fr, TB.kr, a.nbrtab[(size_t)TB.dr * S + s], S);
     }
-    acc.add((R)TA.coef * bc_of<R>(bcm, TA.bcdt, pbc), LA, RA);
+    acc.add((R)TA.coef * bc_of<R>(bcm, TA.bcdt, pbc) * ((LF ? TA.kl : TA.kr) ? (R)1 : a.eta_scale),
+              LA, RA);
     if (!hb) break;
     const bool ha = t + 2 < t1;
     if (ha) {
@@ -258,7 +262,8 @@ SUSY_D void run_pattern_pp(ACC& acc, const FopArgs<R>& a, int s, unsigned bcm, i
       LA = ldm<N, R, AL>(fl, TA.kl, a.nbrtab[(size_t)TA.dl * S + s], S);
       RA = ldm<N, R, AR>(fr, TA.kr, a.nbrtab[(size_t)TA.dr * S + s], S);
     }
-    acc.add((R)TB.coef * bc_of<R>(bcm, TB.bcdt, pbc), LB, RB);
+    acc.add((R)TB.coef * bc_of<R>(bcm, TB.bcdt, pbc) * ((LF ? TB.kl : TB.kr) ? (R)1 : a.eta_scale),
+              LB, RB);
     if (!ha) break;
   }
 }

@@ -22,6 +22,8 @@ struct FopArgs {
   int comp_major;   // block order: 1 = all blocks of one output component together
   int nsb;          // site blocks per component
   const int* nbrtab;  // neighbour index table of the table-driven variant
+  R eta_scale;        // 2 with the reference's RESCALE (the site component of
+                      // input and output doubled, utilities.c:795,841), else 1
 };
 
 constexpr int FOP_THREADS = 128;

@@ -187,7 +187,8 @@ SUSY_D void det_stol_rt(Mat<N, R>& acc, const FopArgs<R>& a, const Site& c, int 
     const Cx<R> trm = ldtr<N, R, ADJ>(a.src, 0, mE, S);
     tsum = tsum + bcf<R>(g, c, -et(e)) * (trm * ldc<R>(a.pd + (size_t)(B * 5 + e) * S + mE));
   }
-  const Cx<R> f = ((R)(-0.5) * a.G) * tsum;
+  // every term carries Tr eta, doubled with the reference's RESCALE
+  const Cx<R> f = ((R)(-0.5) * a.G * a.eta_scale) * tsum;
   const typename CT<R>::T* pu = a.Uinv + (size_t)(B * N * N) * S + s;
 #pragma unroll
   for (int i = 0; i < N; i++)
@@ -225,6 +226,17 @@ SUSY_D void det_ltos_rt(Mat<N, R>& acc, const FopArgs<R>& a, const Site& c) {
   for (int i = 0; i < N; i++) acc.e[i][i] = acc.e[i][i] + d;
 }
 
+// The reference's RESCALE doubles the site component of the output
+// (utilities.c:841-844)
+template <int N, typename R>
+SUSY_D void eta_rescale(Mat<N, R>& acc, R sc) {
+  if (sc == (R)1) return;
+#pragma unroll
+  for (int i = 0; i < N; i++)
+#pragma unroll
+    for (int j = 0; j < N; j++) acc.e[i][j] = sc * acc.e[i][j];
+}
+
 // Shared epilogue: determinant terms, adjoint for D^dag, axpy and dot
 template <int N, typename R, int SIGN>
 SUSY_D double fop_finish(Mat<N, R>& acc, const FopArgs<R>& a, const Site& c, int comp) {
@@ -234,6 +246,7 @@ SUSY_D double fop_finish(Mat<N, R>& acc, const FopArgs<R>& a, const Site& c, int
     else if (comp <= NUMLINK)
       det_stol_rt<N, R, SIGN>(acc, a, c, comp - 1);
   }
+  if (comp == 0) eta_rescale(acc, a.eta_scale);
   if (SIGN < 0) {
     Mat<N, R> t = acc;
 #pragma unroll

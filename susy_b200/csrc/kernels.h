@@ -56,8 +56,8 @@ struct MsVecs {
 // (P[0] a copy of the operator input p0 at that point); x[j] the solutions.
 // p0_32 / mp32: FP32 operator input and output when the operator runs in
 // FP32 (p0_32 written by the p0 update; nullptr in FP64).
-// f32 = 1: ring, P and p0 are FP32 fields (the operator's input is p0
-// itself, its output mp32); the solutions x stay FP64.
+// f32 = 1: ring and p0 are FP32 fields (the operator's input is p0 itself,
+// its output mp32); the search vectors P and the solutions x stay FP64.
 struct MsBlockVecs {
   void* ring[MS_BLK + 1];
   void* P[MS_MAXS];
@@ -94,7 +94,8 @@ enum { FOP_MAT = 0, FOP_MAT_CM = 1, FOP_ROWS = 2, FOP_COMPACT = 3, FOP_COMPACT_P
 template <typename R>
 int fermion_op(const Geo& g, int N, const void* U, const void* Uinv, const void* pd,
                 const void* src, void* dst, int sign, double G, const void* add, double addc,
-                double* dot, const int* skip, int variant, const int* nbrtab, cudaStream_t st);
+                double* dot, const int* skip, int variant, const int* nbrtab, cudaStream_t st,
+                double eta_scale = 1.0);
 template <typename R> struct FopArgs;
 template <typename R>
 int fermion_op_rows(const FopArgs<R>& a, int N, int sign, cudaStream_t st);

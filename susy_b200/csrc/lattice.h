@@ -36,14 +36,15 @@ struct susy_b200_lattice {
   std::vector<void*> pvec64;  // p_j of the FP64 multi-shift CG
   std::vector<void*> pvec32;
   std::vector<void*> ring;    // residual ring of the blocked FP64 solver
-  std::vector<void*> vec32;   // FP32 ring and search vectors of the mixed solver's FP32 phase
-  int mix_vec32 = 1;          // mixed solver: FP32 vectors in its FP32 phase
+  std::vector<void*> vec32;   // FP32 residual ring of the mixed solver's FP32 phase
+  int mix_vec32 = 0;          // mixed solver: FP32 residuals and p0 in its FP32 phase
+  int rescale = 0;            // the reference's RESCALE: eta doubled in and out of fermion_op
   double* meas = nullptr;     // measurement partials
   size_t meas_n = 0;
   int ms_blocked = 1;         // FP64 multi-shift CG: blocked vector update
   int use_graphs = 1;         // replay the solver's iteration chunks as CUDA graphs
   int host_solver = 0;        // solver behind susy_b200_congrad_multi
-  double mix_switch = 3e-5;   // mixed solver: FP32 operator once |r| < this |src|
+  double mix_switch = 3e-4;   // mixed solver: FP32 operator once |r| < this |src|
   double mix_reliable = 1e-2; // mixed solver: true residual when |r| fell this much
   int mix_correct32 = 1;      // mixed solver: per-shift corrections with the FP32 operator
   std::vector<void*> extra;   // other lazily allocated fields

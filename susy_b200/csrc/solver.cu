@@ -2,7 +2,7 @@
 //
 // multishift_fp64   the reference's congrad_multi in FP64 throughout.
 // multishift_mixed  (1) the same multi-shift recurrences (blocked update)
-//                   with the operator in FP32 once |r| < 3e-5 |src| and
+//                   with the operator in FP32 once |r| < 3e-4 |src| and
 //                   FP64 reliable updates of the base residual;
 //                   (2) per shift, the FP64 true residual
 //                   r = b - (D^dag D + sigma) x; a shift with
@@ -116,8 +116,7 @@ static void* ring_field(susy_b200_lattice* h, int q) {
   return h->ring[q];
 }
 
-// FP32 fields of the mixed solver's FP32 phase: residual ring slots
-// 0..MS_BLK, then the search vectors P_j at MS_BLK + 1 + j
+// FP32 residual ring slots 0..MS_BLK of the mixed solver's FP32 phase
 static void* vec32_field(susy_b200_lattice* h, int q) {
   while ((int)h->vec32.size() <= q) h->vec32.push_back(dalloc(h, field_bytes(h, NTF, 32)));
   return h->vec32[q];
@@ -177,10 +176,10 @@ static double true_residual(susy_b200_lattice* h, const void* b, const void* x, 
 //
 // mixed = false: FP64 throughout (the reference's solver).
 // mixed = true: the operator runs in FP64 until |r| < mix_switch |src|
-// (handle setting, default 3e-5) and in FP32 after that; with mix_vec32
-// (the default) the residual ring, the search vectors and the operator's
-// input are FP32 fields from then on too (half the vector traffic of the
-// FP32 phase), while the recurrences and the solutions stay FP64.  Once the operator is FP32,
+// (handle setting, default 3e-4) and in FP32 after that; with mix_vec32
+// (the default) the residual ring and the operator's input are FP32 fields
+// from then on too, while the recurrences, the shifted search vectors and
+// the solutions stay FP64.  Once the operator is FP32,
 // the iterated residual drifts from the true one by the FP32 rounding of
 // each product, so at block boundaries, whenever |r| fell by mix_reliable
 // (default 1e-2) since the last check and when the solve stops, the FP64
@@ -190,11 +189,12 @@ static double true_residual(susy_b200_lattice* h, const void* b, const void* x, 
 // products enter only when the residual is small, so the shifted systems,
 // which never see a residual replacement, keep an error of order FP32
 // rounding times that residual.  Switching earlier costs more in the
-// per-shift correction solves than it saves: measured at 12^3 x 24 U(3),
-// switching at 1e-3 took 894 iterations in all, at 3e-4 588 (FP64: 567);
-// in full trajectories, whose solves run ~2200 iterations, the corrections
-// after a switch at 3e-4 cost more than the FP32 operator saved, and 3e-5
-// was the fastest of 3e-4 ... 1e-5.
+// per-shift correction solves than it saves.  On the thermalised 12^3 x 24
+// U(3) benchmark configuration (FP64: 3128 iterations) |r| stays near
+// 1e-3 ... 1e-2 |src| for the first ~1700 iterations before it falls at
+// ~130 iterations per decade, so the FP32 operator can only take the last
+// ~40% of the solve: switching at 1e-3 took 4653 iterations in all, at
+// 3e-4 3184 (1.11x faster than FP64), 1e-4 3175, 3e-5 3169, 1e-6 3157.
 
 static int ms_run_block(susy_b200_lattice* h, const void* src, void* const* psim, int norder,
                         const double* shift, int MaxCG, double errormin, bool mixed,
@@ -317,21 +317,18 @@ static int ms_run_block(susy_b200_lattice* h, const void* src, void* const* psim
         fp32_op = true;
         convert_field(n, p0, 64, p0_32, 32, s);
         if (h->mix_vec32) {
-          // FP32 vectors from here on (this poll follows a block pass, so
-          // the search vectors are current and the residual of this
-          // iteration is the only ring slot the next steps read): the
-          // operator's input is the FP32 p0 itself; the solutions stay FP64
+          // FP32 residuals from here on (this poll follows a block pass,
+          // so the residual of this iteration is the only ring slot the
+          // next steps read), and the operator's input is the FP32 p0
+          // itself.  The shifted search vectors and the solutions stay
+          // FP64: rounding P_j to FP32 every block puts an error of order
+          // u_32 |P_j| (not u_32 |r|) into every shifted system, which
+          // measured 8x the per-shift correction iterations.
           const int slot = pw[1] % (MS_BLK + 1);
           for (int q = 0; q <= MS_BLK; q++)
             if (!vec32_field(h, q)) return set_err(h, SUSY_B200_ENOMEM);
           convert_field(n, v.ring[slot], 64, vec32_field(h, slot), 32, s);
           for (int q = 0; q <= MS_BLK; q++) v.ring[q] = vec32_field(h, q);
-          for (int j = 0; j < norder; j++) {
-            void* p32 = vec32_field(h, MS_BLK + 1 + j);
-            if (!p32) return set_err(h, SUSY_B200_ENOMEM);
-            convert_field(n, v.P[j], 64, p32, 32, s);
-            v.P[j] = p32;
-          }
           v.p0 = p0_32;
           v.f32 = 1;
         } else {

@@ -166,6 +166,8 @@ def load_library(path: str = LIB_PATH):
     L.susy_b200_pf_streams.argtypes = [_vp, C.c_int]
     L.susy_b200_cg_blocked.restype = C.c_int
     L.susy_b200_cg_blocked.argtypes = [_vp, C.c_int]
+    L.susy_b200_set_rescale.restype = C.c_int
+    L.susy_b200_set_rescale.argtypes = [_vp, C.c_int]
     L.susy_b200_mixed_vectors.restype = C.c_int
     L.susy_b200_mixed_vectors.argtypes = [_vp, C.c_int]
     L.susy_b200_cg_freeze_iterations.restype = C.c_int
@@ -435,7 +437,7 @@ class Lattice:
     def autotune(self):
         self._check(self.lib.susy_b200_autotune(self.h))
 
-    def mixed_params(self, fp32_below: float = 3e-5, reliable_factor: float = 1e-2):
+    def mixed_params(self, fp32_below: float = 3e-4, reliable_factor: float = 1e-2):
         """Mixed solver: FP32 operator once |r| < fp32_below |src|; FP64
         residual replacement whenever |r| fell by reliable_factor."""
         self._check(self.lib.susy_b200_mixed_params(self.h, float(fp32_below),
@@ -445,6 +447,11 @@ class Lattice:
         """Mixed solver: per-shift correction solves with the FP32 operator
         (iterative refinement against the FP64 true residual) or in FP64."""
         self._check(self.lib.susy_b200_mixed_correction(self.h, 1 if fp32 else 0))
+
+    def set_rescale(self, on: int = -1) -> int:
+        """The reference's RESCALE option (the site component of the
+        operator's input and output doubled); returns the previous setting."""
+        return self._check(self.lib.susy_b200_set_rescale(self.h, int(on)))
 
     def mixed_vectors(self, fp32: int = -1) -> int:
         """Mixed solver: FP32 (1) or FP64 (0) ring and search vectors in its

@@ -57,6 +57,10 @@ static void b200_init(void) {
     node0_printf("susy_b200_create failed\n");
     terminate(1);
   }
+#ifdef RESCALE
+  /* the build's RESCALE (defines.h:30) doubles eta in and out of fermion_op */
+  b200_check(susy_b200_set_rescale(H, 1));
+#endif
   node0_printf("susy_b200: hot path on the GPU (libsusy_b200)\n");
 }
 

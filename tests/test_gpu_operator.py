@@ -183,3 +183,37 @@ def test_links_and_momenta_in_place_with_a_site_stride(N):
     assert lib.susy_b200_get_links(lat.h, C.cast(back.ctypes.data + off_link, dp), rec) == 0
     assert lib.susy_b200_get_mom(lat.h, C.cast(back.ctypes.data + off_mom, dp), rec) == 0
     assert np.array_equal(back, buf)
+
+
+@pytest.mark.parametrize("N", [2, 3])
+def test_rescaled_operator(N):
+    """The reference's RESCALE option (eta doubled in and out of fermion_op,
+    utilities.c:795,841): D, D^dag and DSq against the oracle with the same
+    option, FP64 to 1e-13 and the FP32 operator to 1e-5, for every variant
+    the option admits; clearing it restores the plain operator."""
+    from susy_b200.lattice import FOP_NVARIANTS
+    dims = (4, 2, 4, 6)
+    lat, geo, prm, U, der = setup(dims, N, -1, 0.05)
+    prm_r = O.Params(lam=1.0, bmass=0.2, G=0.05, N=N, rescale=True)
+    src = synth.tf_source(dims, N, seed=29)
+    assert lat.set_rescale(1) == 0
+    out = np.zeros(lat.tf_doubles)
+    a, b = lat.tf(64), lat.tf(64)
+    a32, b32 = lat.tf(32), lat.tf(32)
+    a.upload(synth.to_ref(dims, src))
+    lat.dev_convert(a, a32)
+    for v in range(3, FOP_NVARIANTS):
+        lat.fop_variant(64, v)
+        lat.fop_variant(32, v)
+        for sign in (1, -1):
+            want = O.fermion_op(geo, prm_r, U, der, src, sign)
+            lat.fermion_op(synth.to_ref(dims, src), out, sign)
+            assert rel(synth.from_ref(dims, out, 16, N), want) < FP64_TOL, (v, sign)
+            lat.dev_fermion_op(a32, b32, sign)
+            lat.dev_convert(b32, b)
+            assert rel(synth.from_ref(dims, b.download(), 16, N), want) < FP32_TOL, (v, sign)
+        lat.DSq(synth.to_ref(dims, src), out)
+        assert rel(synth.from_ref(dims, out, 16, N), O.DSq(geo, prm_r, U, der, src)) < FP64_TOL
+    assert lat.set_rescale(0) == 1
+    lat.fermion_op(synth.to_ref(dims, src), out, 1)
+    assert rel(synth.from_ref(dims, out, 16, N), O.fermion_op(geo, prm, U, der, src, 1)) < FP64_TOL

@@ -79,3 +79,57 @@ def test_reference_program_with_the_shim_reproduces_its_regression_output(N, tmp
         assert not mismatches(have, want)
     for tag, vals in gold["start_meas"].items():
         assert not mismatches({tag: got["start_meas"][tag]}, {tag: vals})
+
+
+def run_app(prog, N, tmp_path):
+    """Run the reference's susy_<prog> linked with the shim on its regression
+    input; returns the parsed output and the golden."""
+    from susy_b200 import io_lat
+    exe = os.path.join(ROOT, "oracle", "_ref", "n%d%s" % (N, prog), "susy_%s_b200" % prog)
+    if not os.path.exists(exe):
+        pytest.skip("shimmed susy_%s not built (oracle/build_ref.sh %s%d needs the "
+                    "reference sources)" % (prog, prog, N))
+    gold = json.load(open(os.path.join(GOLD, "%s_U%d.json" % (prog, N))))
+    cfg = np.load(os.path.join(GOLD, "config_U%d_4444.npz" % N))
+    dims = tuple(int(x) for x in cfg["dims"])
+    conf = dict(gold["input"])["reload_serial"]
+    io_lat.write_gauge(str(tmp_path / conf), dims, cfg["links"].astype(np.complex128))
+    text = "\n".join("%s %s" % (k, v) for k, v in gold["input"]) + "\nforget\n"
+    run = subprocess.run([exe], input=text, cwd=str(tmp_path), capture_output=True, text=True,
+                         timeout=900)
+    assert run.returncode == 0, run.stdout[-2000:] + run.stderr[-2000:]
+    assert "susy_b200: hot path on the GPU" in run.stdout
+    spec = importlib.util.spec_from_file_location("ma", os.path.join(GOLD, "make_golden_apps.py"))
+    ma = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(ma)
+    return ma.parse_output(run.stdout), gold
+
+
+@pytest.mark.parametrize("N", [2, 3])
+def test_reference_chebyshev_program_with_the_shim(N, tmp_path):
+    """susy_cheb (chebyshev.c:45,60 apply DSq to stochastic sources) with
+    DSq from the library reproduces cheb.U<N>.ref: every Chebyshev
+    coefficient to its printed 8 digits, its error to its 4 digits."""
+    got, gold = run_app("cheb", N, tmp_path)
+    assert len(got["chebyshev"]) == len(gold["chebyshev"]) > 0
+    for g, w in zip(got["chebyshev"], gold["chebyshev"]):
+        assert g[0] == w[0]
+        assert abs(g[1] - w[1]) <= 3e-7 * abs(w[1]) + 1e-12, (g, w)
+        assert abs(g[2] - w[2]) <= 3e-3 * abs(w[2]) + 1e-12, (g, w)
+
+
+@pytest.mark.parametrize("N", [2, 3])
+def test_reference_mode_number_program_with_the_shim(N, tmp_path):
+    """susy_mode (modenumber.c:26,63,66 call congrad_multi on stochastic
+    sources, error_per_site 1e-5) with congrad_multi from the library
+    reproduces mode.U<N>.ref: the step-function line exactly, every mode
+    number to 1e-5 relative (the solves stop at a residual of 1e-5 per
+    site, and the solver's summation order may move the stop by an
+    iteration), its error to its printed 4 digits."""
+    got, gold = run_app("mode", N, tmp_path)
+    assert got["step"] == gold["step"]
+    assert len(got["mode"]) == len(gold["mode"]) > 0
+    for g, w in zip(got["mode"], gold["mode"]):
+        assert g[0] == w[0]
+        assert abs(g[1] - w[1]) <= 1e-5 * abs(w[1]), (g, w)
+        assert abs(g[2] - w[2]) <= 3e-3 * abs(w[2]) + 1e-12, (g, w)
