@@ -717,6 +717,108 @@ def run_traj_case(args):
                       "runs": out}), flush=True)
 
 
+def run_learned_case(args):
+    """The learned-preconditioner protocol of the benchmark's fourth
+    configuration on one lattice (default 8^4 U(2); --dims / --ncol),
+    lambda 1, bmass 0.2, G 0.05:
+      chain   near-identity links (noise 0.2, seed 31), 200 RHMC
+              trajectories (Nroot 1, degree 15, 10 x 2 steps, length 1,
+              error_per_site 1e-5), every 5th saved: 40 configurations;
+      pairs   --learned-pairs (100) per configuration, r complex Gaussian,
+              e = (D^dag D + sigma_0)^-1 r by the FP64 solver (sigma_0 the
+              smallest shift4 pole of Nroot 2), 30 configurations train, 10
+              are held out;
+      train   Adam on the A-norm error (the quantity CG minimises),
+              --learned-steps steps of --learned-batch pairs;
+      eval    on each held-out configuration one Gaussian source, the 15
+              shift4 poles to the FP64 true residual 1e-10 per site: the
+              FP64 multi-shift, the mixed solver, and a multi-shift pass to
+              1e-6 followed by flexible CG on the 4 smallest shifts with
+              and without the network (tensor-core inference).
+    Prints one JSON line per held-out configuration and a summary."""
+    import torch
+    from susy_b200 import Lattice, RHMC, synth
+    from susy_b200.learned import Net, congrad_multi_learned, make_pairs
+    from susy_b200.rhmc_tables import rhmc
+    dims = tuple(int(x) for x in args.dims.split(",")) if args.dims else (8, 8, 8, 8)
+    ncol = args.ncol or 2
+    lat = Lattice(dims, ncol, pbc=-1, lam=1.0, bmass=0.2, G=0.05, iseed=31)
+    st = torch.cuda.Stream()
+    lat.set_stream(st.cuda_stream)
+    lat.set_links(synth.to_ref(dims, synth.links(dims, ncol, 0.2, 31)))
+    chain = RHMC(15, 1, nstep=10, nstep_gauge=2, traj_length=1.0, error_per_site=1e-5)
+    t0 = time.time()
+    configs, acc = [], 0
+    for i in range(1, 201):
+        acc += int(lat.update(chain)["accept"])
+        if i % 5 == 0:
+            configs.append(lat.get_links())
+    t_chain = time.time() - t0
+    shifts = np.array(rhmc(15, 2)["shift4"])
+    sigma0 = float(shifts[0])
+    t0 = time.time()
+    pairs = []
+    for c, links in enumerate(configs[:30]):
+        lat.set_links(links)
+        for r, e in make_pairs(lat, sigma0, args.learned_pairs, seed=10000 + 1000 * c):
+            pairs.append((r, e, links))
+    t_pairs = time.time() - t0
+    lat.set_links(configs[0])
+    net = Net(lat)
+    t0 = time.time()
+    hist = net.train(pairs, steps=args.learned_steps, lr=2e-3, batch=args.learned_batch,
+                     sigma=sigma0, log=max(1, args.learned_steps // 10))
+    t_train = time.time() - t0
+    del pairs
+    print(json.dumps({"case": "learned_train", "lattice": "x".join(map(str, dims)), "ncol": ncol,
+                      "trajectories": 200, "accepted": acc, "configs": len(configs),
+                      "train_pairs": 30 * args.learned_pairs, "sigma0": sigma0,
+                      "loss_first": hist[0], "loss_last10": float(np.mean(hist[-10:])),
+                      "chain_s": t_chain, "pairs_s": t_pairs, "train_s": t_train}), flush=True)
+
+    def timed(fn):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        out = fn()
+        e1.record(st)
+        e1.synchronize()
+        return out, e0.elapsed_time(e1)
+
+    rows = []
+    for c, links in enumerate(configs[30:]):
+        lat.set_links(links)
+        src = lat.tf(64)
+        src.upload(synth.to_ref(dims, synth.tf_source(dims, ncol, 50000 + c)))
+        b2 = float(np.dot(src.download(), src.download()))
+        psim = [lat.tf(64) for _ in shifts]
+        row = {"case": "learned_heldout", "config": 30 + c}
+        lat.dev_congrad_multi(src, psim, shifts, 50000, 1e-20)     # warm-up
+        (it, _), ms = timed(lambda: lat.dev_congrad_multi(src, psim, shifts, 50000, 1e-20))
+        row["fp64"] = {"iterations": it, "ms": ms}
+        (it, _), ms = timed(lambda: lat.dev_congrad_multi(src, psim, shifts, 50000, 1e-20,
+                                                          mixed=True))
+        row["mixed"] = {"iterations": it, "ms": ms}
+        for name, nn in (("refine_plain", None), ("refine_learned", net)):
+            res, ms = timed(lambda: congrad_multi_learned(lat, nn, src, psim, shifts, 50000,
+                                                           1e-20, nrefine=4, loose=1e-12))
+            it, rit, worst = res
+            row[name] = {"iterations": it, "refine_iterations": rit, "ms": ms,
+                         "true_residual_rel_max": worst / b2}
+        rows.append(row)
+        print(json.dumps(row), flush=True)
+    summ = {k: {"iterations": float(np.mean([r[k]["iterations"] for r in rows])),
+                "ms": float(np.mean([r[k]["ms"] for r in rows]))}
+            for k in ("fp64", "mixed", "refine_plain", "refine_learned")}
+    for k in ("refine_plain", "refine_learned"):
+        summ[k]["refine_iterations"] = float(np.mean([r[k]["refine_iterations"] for r in rows]))
+    print(json.dumps({"case": "learned_summary", "lattice": "x".join(map(str, dims)),
+                      "ncol": ncol, "heldout": len(rows), "mean": summ,
+                      "learned_vs_fp64": summ["fp64"]["ms"] / summ["refine_learned"]["ms"],
+                      "learned_vs_plain_refinement":
+                          summ["refine_plain"]["ms"] / summ["refine_learned"]["ms"]}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -739,6 +841,12 @@ def main():
                     help="with --traj-case: comma list of mixed, mixed_fp64_corrections, fp64")
     ap.add_argument("--traj-case", action="store_true",
                     help="full RHMC trajectories of the bench lattice, mixed and FP64 solver")
+    ap.add_argument("--learned-case", action="store_true",
+                    help="the learned-preconditioner protocol: chain, pairs, training, "
+                         "held-out solves")
+    ap.add_argument("--learned-pairs", type=int, default=100)
+    ap.add_argument("--learned-steps", type=int, default=300)
+    ap.add_argument("--learned-batch", type=int, default=8)
     ap.add_argument("--lattices", type=int, default=48)
     ap.add_argument("--threads", type=int, default=48)
     args = ap.parse_args()
@@ -750,6 +858,9 @@ def main():
         return
     if args.traj_case:
         run_traj_case(args)
+        return
+    if args.learned_case:
+        run_learned_case(args)
         return
 
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -373,6 +373,12 @@ susy_b200_net *susy_b200_net_create(susy_b200_lattice *h);
 void susy_b200_net_destroy(susy_b200_net *n);
 int susy_b200_net_set_weights(susy_b200_net *n, const double *w);
 int susy_b200_net_apply(susy_b200_net *n, const void *src, void *dst);
+/* net_apply's channel mixes: on the tensor cores (on = 1, the default; the
+ * transports rounded to bfloat16, mma.sync BF16 x BF16 products with FP32
+ * accumulation) or as FP32 multiply-adds (on = 0).  Training
+ * (net_loss_grad*) always runs the FP32 forward pass it differentiates.
+ * on < 0 only queries; returns the previous setting. */
+int susy_b200_net_tensor_cores(susy_b200_net *n, int on);
 /* loss = |N(r) - e|^2 / |e|^2 for device Twist_Fermions r, e; when grad is
  * not NULL, grad += dL/dW* (complex interleaved, the layout of set_weights:
  * dL/dRe w = 2 Re, dL/dIm w = 2 Im) */

@@ -125,11 +125,17 @@ def init_weights(seed=0, scale=1e-2):
     return Ws
 
 
-def forward(geo, U, Uinv, Ws, tf, keep=False):
+def forward(geo, U, Uinv, Ws, tf, keep=False, bf16_act=False):
+    """bf16_act: the transports are rounded to bfloat16 (real and imaginary
+    parts, nearest even) before each channel mix, as the device's
+    tensor-core inference path feeds them to its BF16 matrix multiplies
+    (FP32 accumulation)."""
     X = embed(geo, U, Uinv, tf)
     acts = []
     for W in Ws:
         T = transports(geo, U, Uinv, X)
+        if bf16_act:
+            T = bf16(T.astype(np.complex64))
         acts.append(T)
         X = layer(T, W)
     out = unembed(geo, U, X)

@@ -259,6 +259,63 @@ __global__ void __launch_bounds__(LT) k_mix_adj(long M, int K, const float2* gOu
   }
 }
 
+// Channel mixing on the tensor cores (inference): the complex product
+// out[c][r] = sum_k W[k][c] T[k][r] as the real GEMM
+//   [M rows x 2K] x [2K x 2 Cout],  A[r][2k + p] = (Re, Im)_p T[k][r],
+//   B[2k + p][2c + q] = {{Re W, Im W}, {-Im W, Re W}}[p][q],
+// with mma.m16n8k16 (BF16 inputs, FP32 accumulation).  With (Re, Im) of a
+// complex element adjacent along K, every A-fragment register of a thread
+// is one transport element T[k][r] rounded to a bf16 pair, and every pair
+// of accumulator registers is (Re, Im) of one output channel.  The B
+// fragments are packed by the host (net_set_weights) in the order a warp
+// reads them: Wp[(step * NT + tile) * 32 + lane] = {b0, b1}.  One warp per
+// 16 rows, all output channels; rows past M read zeros and store nothing.
+SUSY_D uint32_t bf16x2(float2 v) {
+  const __nv_bfloat162 b = __floats2bfloat162_rn(v.x, v.y);
+  uint32_t u;
+  memcpy(&u, &b, 4);
+  return u;
+}
+
+template <int COUT>
+__global__ void __launch_bounds__(128) k_mix_mma(long M, int K, const float2* T, const uint2* Wp,
+                                                 float2* out) {
+  constexpr int NT = COUT / 4;        // n8 tiles of the 2 COUT real columns
+  const int lane = threadIdx.x & 31, gid = lane >> 2, tig = lane & 3;
+  const long r0 = ((long)blockIdx.x * 4 + (threadIdx.x >> 5)) * 16;
+  if (r0 >= M) return;
+  const long ra = r0 + gid, rb = r0 + gid + 8;
+  const bool oka = ra < M, okb = rb < M;
+  float acc[NT][4];
+#pragma unroll
+  for (int t = 0; t < NT; t++) acc[t][0] = acc[t][1] = acc[t][2] = acc[t][3] = 0.f;
+  const float2 z = make_float2(0.f, 0.f);
+  const int steps = K / 8;            // 16 real K values = 8 complex ones per step
+#pragma unroll 1
+  for (int st = 0; st < steps; st++) {
+    const float2* t0 = T + (size_t)(8 * st + tig) * M;
+    const float2* t4 = T + (size_t)(8 * st + tig + 4) * M;
+    const uint32_t a0 = bf16x2(oka ? t0[ra] : z), a1 = bf16x2(okb ? t0[rb] : z);
+    const uint32_t a2 = bf16x2(oka ? t4[ra] : z), a3 = bf16x2(okb ? t4[rb] : z);
+    const uint2* wp = Wp + (size_t)st * NT * 32 + lane;
+#pragma unroll
+    for (int t = 0; t < NT; t++) {
+      const uint2 b = __ldg(wp + t * 32);
+      asm volatile(
+          "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 "
+          "{%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, {%0, %1, %2, %3};\n"
+          : "+f"(acc[t][0]), "+f"(acc[t][1]), "+f"(acc[t][2]), "+f"(acc[t][3])
+          : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b.x), "r"(b.y));
+    }
+  }
+#pragma unroll
+  for (int t = 0; t < NT; t++) {
+    const int c = 4 * t + tig;
+    if (oka) out[(size_t)c * M + ra] = make_float2(acc[t][0], acc[t][1]);
+    if (okb) out[(size_t)c * M + rb] = make_float2(acc[t][2], acc[t][3]);
+  }
+}
+
 // partial[rb][k][c] = sum over rows of chunk rb of conj(T[k][r]) g[c][r]
 template <int COUT>
 __global__ void __launch_bounds__(LT) k_wgrad(long M, int K, const float2* T, const float2* gOut,
@@ -333,6 +390,8 @@ static const int kChan[4] = {16, 32, 32, 16};
 struct susy_b200_net {
   susy_b200_lattice* h = nullptr;
   uint32_t* W[3] = {};            // bf16 pairs, [11 Cin][Cout] per layer
+  uint2* Wp[3] = {};              // the same weights as k_mix_mma's B fragments
+  int tc = 1;                     // net_apply mixes on the tensor cores
   float2* X[4] = {};              // channel fields: input of each layer, output
   float2* T[3] = {};              // transports of each layer's input
   float2* gA = nullptr;           // gradient w.r.t. a layer's output / input
@@ -349,6 +408,8 @@ struct susy_b200_net {
 static long net_rows(const susy_b200_lattice* h) { return (long)h->N * h->N * h->g.S; }
 
 static int net_kw(int l) { return NT_TAP * kChan[l] * kChan[l + 1]; }
+// B-fragment entries of layer l (uint2 each): K / 8 steps x Cout / 4 tiles x 32 lanes
+static size_t net_kwp(int l) { return (size_t)(NT_TAP * kChan[l] / 8) * (kChan[l + 1] / 4) * 32; }
 
 extern "C" int susy_b200_net_nweights(void) { return net_kw(0) + net_kw(1) + net_kw(2); }
 
@@ -360,6 +421,8 @@ extern "C" susy_b200_net* susy_b200_net_create(susy_b200_lattice* h) {
   bool ok = true;
   for (int l = 0; l < 3; l++) {
     n->W[l] = (uint32_t*)dalloc(h, (size_t)net_kw(l) * sizeof(uint32_t));
+    n->Wp[l] = (uint2*)dalloc(h, net_kwp(l) * sizeof(uint2));
+    ok = ok && n->Wp[l];
     n->T[l] = (float2*)dalloc(h, (size_t)NT_TAP * kChan[l] * M * sizeof(float2));
     ok = ok && n->W[l] && n->T[l];
   }
@@ -390,6 +453,7 @@ extern "C" void susy_b200_net_destroy(susy_b200_net* n) {
   if (!n) return;
   for (int l = 0; l < 3; l++) {
     if (n->W[l]) cudaFree(n->W[l]);
+    if (n->Wp[l]) cudaFree(n->Wp[l]);
     if (n->T[l]) cudaFree(n->T[l]);
   }
   for (int l = 0; l < 4; l++)
@@ -426,14 +490,40 @@ extern "C" int susy_b200_net_set_weights(susy_b200_net* n, const double* w) {
         }
     cudaMemcpyAsync(n->W[l], hw.data(), hw.size() * sizeof(uint32_t), cudaMemcpyHostToDevice,
                     n->h->stream);
+    // B fragments of k_mix_mma: lane (gid, tig) of tile t, step st holds
+    // B[2k + p][nr], nr = 8 t + gid (output channel nr / 2, Re or Im by
+    // nr % 2), k = 8 st + tig (b0) and + 4 (b1), p = 0, 1 in the low and
+    // high halves; B = {{Re W, Im W}, {-Im W, Re W}}[p][nr % 2]
+    const int steps = NT_TAP * ci / 8, nt = co / 4;
+    std::vector<uint2> hp(net_kwp(l));
+    auto wpair = [&](int kk, int d, int q) -> uint32_t {
+      const int k = kk / ci, c = kk % ci;
+      const size_t src = off + 2 * (((size_t)k * co + d) * ci + c);
+      const uint16_t wr = to_bf16((float)w[src]), wi = to_bf16((float)w[src + 1]);
+      const uint16_t lo = q ? wi : wr;
+      const uint16_t hi = q ? wr : (uint16_t)(wi ^ 0x8000u);
+      return (uint32_t)lo | ((uint32_t)hi << 16);
+    };
+    for (int st = 0; st < steps; st++)
+      for (int t = 0; t < nt; t++)
+        for (int lane = 0; lane < 32; lane++) {
+          const int gid = lane >> 2, tig = lane & 3, nr = 8 * t + gid;
+          uint2 b;
+          b.x = wpair(8 * st + tig, nr >> 1, nr & 1);
+          b.y = wpair(8 * st + tig + 4, nr >> 1, nr & 1);
+          hp[((size_t)st * nt + t) * 32 + lane] = b;
+        }
+    cudaMemcpyAsync(n->Wp[l], hp.data(), hp.size() * sizeof(uint2), cudaMemcpyHostToDevice,
+                    n->h->stream);
     if (!ck(n->h, cudaStreamSynchronize(n->h->stream))) return SUSY_B200_ECUDA;
     off += 2 * (size_t)net_kw(l);
   }
   return SUSY_B200_OK;
 }
 
+// tc: channel mixes on the tensor cores (BF16 transports) or in FP32
 template <int N>
-static void forward_n(susy_b200_net* n, const void* src, void* dst) {
+static void forward_n(susy_b200_net* n, const void* src, void* dst, bool tc) {
   susy_b200_lattice* h = n->h;
   const Geo& g = h->g;
   const int nb = (g.V + LT - 1) / LT;
@@ -446,7 +536,12 @@ static void forward_n(susy_b200_net* n, const void* src, void* dst) {
     count_launch(), k_transport<N><<<dim3(nb, kChan[l]), LT, 0, s>>>(
         g, (const float2*)h->U32, (const float2*)h->Uinv32, n->X[l], kChan[l], n->T[l]);
     const int K = NT_TAP * kChan[l];
-    if (kChan[l + 1] == 32)
+    const int wb = (int)((M + 63) / 64);   // 4 warps of 16 rows per block
+    if (tc && kChan[l + 1] == 32)
+      count_launch(), k_mix_mma<32><<<wb, 128, 0, s>>>(M, K, n->T[l], n->Wp[l], n->X[l + 1]);
+    else if (tc)
+      count_launch(), k_mix_mma<16><<<wb, 128, 0, s>>>(M, K, n->T[l], n->Wp[l], n->X[l + 1]);
+    else if (kChan[l + 1] == 32)
       count_launch(), k_mix<32><<<mb, LT, 0, s>>>(M, K, n->T[l], n->W[l], n->X[l + 1]);
     else
       count_launch(), k_mix<16><<<mb, LT, 0, s>>>(M, K, n->T[l], n->W[l], n->X[l + 1]);
@@ -454,21 +549,28 @@ static void forward_n(susy_b200_net* n, const void* src, void* dst) {
   count_launch(), k_unembed<N><<<nb, LT, 0, s>>>(g, (const float2*)h->U32, n->X[3], (double2*)dst);
 }
 
-static void net_forward(susy_b200_net* n, const void* src, void* dst) {
+static void net_forward(susy_b200_net* n, const void* src, void* dst, bool tc) {
   switch (n->h->N) {
-    case 2: forward_n<2>(n, src, dst); break;
-    case 3: forward_n<3>(n, src, dst); break;
-    default: forward_n<4>(n, src, dst); break;
+    case 2: forward_n<2>(n, src, dst, tc); break;
+    case 3: forward_n<3>(n, src, dst, tc); break;
+    default: forward_n<4>(n, src, dst, tc); break;
   }
 }
 
 namespace susy {
 // z = N(r) on FP64 device Twist_Fermions (used by the preconditioned solver)
 int net_apply(susy_b200_net* n, const void* src, void* dst) {
-  net_forward(n, src, dst);
+  net_forward(n, src, dst, n->tc != 0);
   return ck(n->h, cudaGetLastError()) ? SUSY_B200_OK : SUSY_B200_ECUDA;
 }
 }  // namespace susy
+
+extern "C" int susy_b200_net_tensor_cores(susy_b200_net* n, int on) {
+  if (!n || on > 1) return SUSY_B200_EINVAL;
+  const int prev = n->tc;
+  if (on >= 0) n->tc = on;
+  return prev;
+}
 
 extern "C" int susy_b200_net_apply(susy_b200_net* n, const void* src, void* dst) {
   if (!n || !src || !dst) return SUSY_B200_EINVAL;
@@ -519,7 +621,8 @@ extern "C" int susy_b200_net_loss_grad2(susy_b200_net* n, const void* r, const v
   if (!n || !r || !e || !loss) return SUSY_B200_EINVAL;
   susy_b200_lattice* h = n->h;
   cudaStream_t s = h->stream;
-  net_forward(n, r, n->tfz);
+  // training differentiates the FP32 forward pass
+  net_forward(n, r, n->tfz, false);
   const long nc = tf_complex(h);
   const int db = (int)((nc + 255) / 256);
   count_launch(), k_diff<<<db, 256, 0, s>>>(nc, n->tfz, (const double2*)e, n->tfd, n->part);

@@ -46,6 +46,8 @@ def _setup(L):
     L.susy_b200_net_destroy.argtypes = [_vp]
     L.susy_b200_net_set_weights.restype = C.c_int
     L.susy_b200_net_set_weights.argtypes = [_vp, _dp]
+    L.susy_b200_net_tensor_cores.restype = C.c_int
+    L.susy_b200_net_tensor_cores.argtypes = [_vp, C.c_int]
     L.susy_b200_net_apply.restype = C.c_int
     L.susy_b200_net_apply.argtypes = [_vp, _vp, _vp]
     L.susy_b200_net_loss_grad.restype = C.c_int
@@ -103,6 +105,11 @@ class Net:
         assert v.size == 2 * self.nw
         self.lat._check(self.lib.susy_b200_net_set_weights(self.h, _ptr(v)))
 
+    def tensor_cores(self, on: int = -1) -> int:
+        """Inference mixes on the tensor cores (1, BF16 transports) or in
+        FP32 (0); returns the previous setting."""
+        return self.lat._check(self.lat.lib.susy_b200_net_tensor_cores(self.h, int(on)))
+
     def apply(self, src: DeviceTF, dst: DeviceTF):
         self.lat._check(self.lib.susy_b200_net_apply(self.h, src.ptr, dst.ptr))
 
@@ -117,7 +124,10 @@ class Net:
 
     def train(self, pairs, steps=200, lr=2e-3, batch=8, seed=0, log=None, sigma=-1.0):
         """Adam on the complex weights (FP32 master copy here, bfloat16 on
-        the device) over (r, e) device pairs; returns the loss history."""
+        the device) over (r, e) device pairs; returns the loss history.
+        A pair (r, e, links) also carries its configuration (host links in
+        the reference layout): the lattice is switched to it before the
+        pair's loss is evaluated (a batch is taken config by config)."""
         rng = np.random.default_rng(seed)
         Ws = [W.copy() for W in self.Ws]
         m = [np.zeros_like(W) for W in Ws]
@@ -126,10 +136,14 @@ class Net:
         hist = []
         for t in range(1, steps + 1):
             idx = rng.choice(len(pairs), size=min(batch, len(pairs)), replace=False)
+            idx = sorted(idx, key=lambda i: id(pairs[i][2]) if len(pairs[i]) > 2 else 0)
             tot = 0.0
             gs = [np.zeros_like(W) for W in Ws]
             for i in idx:
-                loss, g = self.loss_grad(*pairs[i], sigma=sigma)
+                if len(pairs[i]) > 2 and getattr(self, "_links_id", None) != id(pairs[i][2]):
+                    self.lat.set_links(pairs[i][2])
+                    self._links_id = id(pairs[i][2])
+                loss, g = self.loss_grad(pairs[i][0], pairs[i][1], sigma=sigma)
                 tot += loss
                 for a, b in zip(gs, g):
                     a += b

@@ -32,11 +32,25 @@ def test_forward_and_gradient_match_the_definition(dims, N):
     dr, de, dz = lat.tf(64), lat.tf(64), lat.tf(64)
     dr.upload(synth.to_ref(dims, r))
     de.upload(synth.to_ref(dims, e))
-    net.apply(dr, dz)
     Ui = np.linalg.inv(U)
     want = Lr.forward(geo, U, Ui, Ws, r)
+    # FP32 channel mixes: the definition to FP32 accuracy
+    assert net.tensor_cores(0) == 1
+    net.apply(dr, dz)
     got = synth.from_ref(dims, dz.download(), 16, N)
     assert np.abs(got - want).max() <= 1e-5 * np.abs(want).max()
+    # tensor-core mixes (BF16 transports, FP32 accumulation): the definition
+    # with the transports rounded to bfloat16; a transport whose FP32 value
+    # sits on a bf16 rounding boundary may round the other way than the
+    # definition's FP64 value does, hence the looser bound
+    net.tensor_cores(1)
+    net.apply(dr, dz)
+    got = synth.from_ref(dims, dz.download(), 16, N)
+    want16 = Lr.forward(geo, U, Ui, Ws, r, bf16_act=True)
+    e16 = np.abs(got - want16).max() / np.abs(want16).max()
+    e32 = np.abs(got - want).max() / np.abs(want).max()
+    print("tensor-core forward: rel. error %.2e vs bf16 definition, %.2e vs FP32" % (e16, e32))
+    assert e16 <= 2e-4
     loss, g = net.loss_grad(dr, de)
     wl, wg = Lr.loss_and_grad(geo, U, Ui, Ws, [r], [e])
     assert abs(loss - wl) <= 1e-5 * wl
