@@ -603,6 +603,113 @@ def run_dsq_case(args):
                   flush=True)
 
 
+# Operator and solver microbenchmark: 8^4 U(2), links identity + 0.2
+# noise, lambda 1, bmass 0.2, G 0.05, antiperiodic in time; 32
+# complex-Gaussian sources; 15 shifts geometrically spaced 1e-5 ... 1e3.
+C1_DIMS, C1_NCOL, C1_SOURCES, C1_DSQ = (8, 8, 8, 8), 2, 32, 1000
+
+
+def run_config1_case(args):
+    """D^dag D applied 1000 times in FP64 and in FP32, cycling over the 32
+    sources (CUDA events on the launching stream; sources and results,
+    2 x 32 x 4.2 MB in FP64, exceed the 126 MB L2, the 1.3 MB of links stay
+    in it): ms per application, algorithmic GB/s and the FP32 result's
+    error against the FP64 one (the FP64 operator itself is pinned to the
+    oracle at 1e-13 on this configuration by the GPU tests).  Then every
+    source solved with the 15 shifts to the FP64 true residual 1e-10 per
+    site by the FP64 solver, the mixed solver at its defaults, and the
+    mixed solver with the FP32 operator from the first iteration and FP64
+    reliable updates every 50 iterations (rounded up to the 8-iteration
+    block): iterations, ms per solve, and per shift the worst FP64 true
+    residual |b - (D^dag D + sigma) x| / |b| and the worst solution error
+    against the FP64 solver's, max |x - x64| / max |x64|."""
+    import torch
+    from susy_b200 import Lattice, synth
+    dims, N = C1_DIMS, C1_NCOL
+    lat = Lattice(dims, N, pbc=-1, lam=1.0, bmass=0.2, G=0.05)
+    st = torch.cuda.Stream()
+    lat.set_stream(st.cuda_stream)
+    lat.set_links(synth.to_ref(dims, synth.links(dims, N, 0.2, 1)))
+    peak, peak_kind = measured_peaks()
+    srcs = [synth.to_ref(dims, synth.tf_source(dims, N, 100 + k)) for k in range(C1_SOURCES)]
+    a64 = [lat.tf(64) for _ in srcs]
+    b64 = [lat.tf(64) for _ in srcs]
+    for a, x in zip(a64, srcs):
+        a.upload(x)
+    a32 = [lat.tf(32) for _ in srcs]
+    b32 = [lat.tf(32) for _ in srcs]
+    for a, c in zip(a64, a32):
+        lat.dev_convert(a, c)
+    ev = lambda: torch.cuda.Event(enable_timing=True)
+    report = {"case": "config1_microbench", "lattice": "x".join(map(str, dims)), "ncol": N,
+              "sources": len(srcs), "dsq_applications": C1_DSQ, "peak_gbs": peak,
+              "peak_kind": peak_kind}
+    for prec, w, A, B in ((64, 16, a64, b64), (32, 8, a32, b32)):
+        for k in range(3):
+            lat.dev_DSq(A[k], B[k])
+        e0, e1 = ev(), ev()
+        e0.record(st)
+        for k in range(C1_DSQ):
+            lat.dev_DSq(A[k % len(A)], B[k % len(B)])
+        e1.record(st)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / C1_DSQ
+        gbs = 2 * algorithmic_bytes_fop(lat.V, N, w) / (ms * 1e-3) / 1e9
+        report["dsq_fp%d" % prec] = {"ms_per_dsq": ms, "algorithmic_gbs": gbs,
+                                     "frac": gbs / peak}
+    t64 = lat.tf(64)
+    err = 0.0
+    for k in range(len(srcs)):
+        lat.dev_DSq(a64[k], b64[k])
+        lat.dev_convert(b32[k], t64)
+        want, got = b64[k].download(), t64.download()
+        err = max(err, float(np.abs(got - want).max() / np.abs(want).max()))
+    report["dsq_fp32_max_rel_err_vs_fp64"] = err
+
+    shifts = synth.geometric_shifts(15, 1e-5, 1e3)
+    psim = [lat.tf(64) for _ in shifts]
+    solvers = (("fp64", False, None), ("mixed", True, (3e-4, 1e-2, 0)),
+               ("fp32_reliable50", True, (1.0, 1e-2, 50)))
+    stats = {name: {"iters": [], "ms": [], "true_res": np.zeros(len(shifts)),
+                    "sol_err": np.zeros(len(shifts))} for name, _, _ in solvers}
+    for k in range(len(srcs)):
+        b = srcs[k]
+        bn = float(np.sqrt(np.dot(b, b)))
+        x64 = None
+        for name, mixed, prm in solvers:
+            if prm:
+                lat.mixed_params(prm[0], prm[1])
+                lat.mixed_reliable_interval(prm[2])
+            e0, e1 = ev(), ev()
+            e0.record(st)
+            it, _ = lat.dev_congrad_multi(a64[k], psim, shifts, MAXCG, ERRORMIN, mixed=mixed)
+            e1.record(st)
+            e1.synchronize()
+            S = stats[name]
+            S["iters"].append(it)
+            S["ms"].append(e0.elapsed_time(e1))
+            xs = [p.download() for p in psim]
+            for j, sg in enumerate(shifts):
+                lat.dev_DSq(psim[j], t64)
+                r = b - t64.download() - sg * xs[j]
+                S["true_res"][j] = max(S["true_res"][j], float(np.sqrt(np.dot(r, r))) / bn)
+                if x64 is not None:
+                    S["sol_err"][j] = max(S["sol_err"][j], float(
+                        np.abs(xs[j] - x64[j]).max() / np.abs(x64[j]).max()))
+            if not mixed:
+                x64 = xs
+    lat.mixed_params()
+    lat.mixed_reliable_interval(0)
+    for name, S in stats.items():
+        report[name] = {"iters_mean": float(np.mean(S["iters"])),
+                        "iters_min": int(min(S["iters"])), "iters_max": int(max(S["iters"])),
+                        "ms_per_solve_mean": float(np.mean(S["ms"])),
+                        "max_true_residual_per_shift": [float(x) for x in S["true_res"]],
+                        "max_sol_err_vs_fp64_per_shift": [float(x) for x in S["sol_err"]]}
+    report["shifts"] = [float(x) for x in shifts]
+    print(json.dumps(report), flush=True)
+
+
 # Batched parameter scan of independent U(2) lattices: volumes from
 # {4^4, 6^4, 8^4, 4^3x8, 6^3x12, 8^3x16}, lambda from {0.5, 1, 2, 4}, link
 # noise 0.1-0.3, all seed-derived; bmass 0.2, G 0.05; degree-15 Nroot 1
@@ -835,6 +942,8 @@ def main():
     ap.add_argument("--variant", type=int, default=-1)
     ap.add_argument("--dims", default="", help="--dsq-case lattice, e.g. 24,24,24,24")
     ap.add_argument("--ncol", type=int, default=0, help="--dsq-case NCOL")
+    ap.add_argument("--config1-case", action="store_true",
+                    help="8^4 U(2) operator and solver microbenchmark, 32 sources")
     ap.add_argument("--batch-case", action="store_true",
                     help="independent U(2) lattices of uneven volume, batched vs one by one")
     ap.add_argument("--traj-solvers", default="",
@@ -852,6 +961,9 @@ def main():
     args = ap.parse_args()
     if args.dsq_case:
         run_dsq_case(args)
+        return
+    if args.config1_case:
+        run_config1_case(args)
         return
     if args.batch_case:
         run_batch_case(args)

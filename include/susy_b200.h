@@ -192,11 +192,18 @@ int susy_b200_pf_streams(susy_b200_lattice *h, int on);
  * Returns the previous setting. */
 int susy_b200_set_solver(susy_b200_lattice *h, int solver);
 /* Mixed-precision solver settings (no reference counterpart): the operator
- * runs in FP32 once |r| < fp32_below |src| (default 3e-4); with the FP32
- * operator the FP64 true residual replaces the iterated one whenever |r|
- * fell by reliable_factor (default 1e-2) since the last replacement.
+ * runs in FP32 once |r| < fp32_below |src| (default 3e-4; fp32_below = 1
+ * runs it in FP32 from the first iteration); with the FP32 operator the
+ * FP64 true residual replaces the iterated one whenever |r| fell by
+ * reliable_factor (default 1e-2) since the last replacement.
  * 0 < fp32_below <= 1, 0 < reliable_factor < 1, else SUSY_B200_EINVAL. */
 int susy_b200_mixed_params(susy_b200_lattice *h, double fp32_below, double reliable_factor);
+/* Mixed solver: iters > 0 replaces the reliable_factor trigger by a fixed
+ * schedule, the FP64 true residual at the first 8-iteration block boundary
+ * at least iters iterations after the previous replacement (or after the
+ * switch to FP32); 0 (default) restores the residual trigger.  iters < 0:
+ * SUSY_B200_EINVAL. */
+int susy_b200_mixed_reliable_interval(susy_b200_lattice *h, int iters);
 /* Mixed solver, after the multi-shift pass: a shift whose FP64 true
  * residual is above the bound gets correction solves (D^dag D + sigma) e = r,
  * x += e, with the FP32 operator and recurrences (fp32 = 1, the default;

@@ -256,6 +256,7 @@ susy_b200_lattice* solver_shadow(susy_b200_lattice* h) {
   c->use_graphs = h->use_graphs;
   c->mix_switch = h->mix_switch;
   c->mix_reliable = h->mix_reliable;
+  c->mix_interval = h->mix_interval;
   c->mix_correct32 = h->mix_correct32;
   c->mix_vec32 = h->mix_vec32;
   c->rescale = h->rescale;
@@ -384,6 +385,12 @@ int susy_b200_mixed_params(susy_b200_lattice* h, double fp32_below, double relia
     return SUSY_B200_EINVAL;
   h->mix_switch = fp32_below;
   h->mix_reliable = reliable_factor;
+  return SUSY_B200_OK;
+}
+
+int susy_b200_mixed_reliable_interval(susy_b200_lattice* h, int iters) {
+  if (!h || iters < 0) return SUSY_B200_EINVAL;
+  h->mix_interval = iters;
   return SUSY_B200_OK;
 }
 

@@ -46,6 +46,7 @@ struct susy_b200_lattice {
   int host_solver = 0;        // solver behind susy_b200_congrad_multi
   double mix_switch = 3e-4;   // mixed solver: FP32 operator once |r| < this |src|
   double mix_reliable = 1e-2; // mixed solver: true residual when |r| fell this much
+  int mix_interval = 0;       // mixed solver: > 0, true residual every this many iterations
   int mix_correct32 = 1;      // mixed solver: per-shift corrections with the FP32 operator
   std::vector<void*> extra;   // other lazily allocated fields
   int* poll = nullptr;        // pinned host words for solver polling

@@ -177,14 +177,15 @@ static double true_residual(susy_b200_lattice* h, const void* b, const void* x, 
 // mixed = false: FP64 throughout (the reference's solver).
 // mixed = true: the operator runs in FP64 until |r| < mix_switch |src|
 // (handle setting, default 3e-4) and in FP32 after that; with mix_vec32
-// (the default) the residual ring and the operator's input are FP32 fields
+// (off by default) the residual ring and the operator's input are FP32 fields
 // from then on too, while the recurrences, the shifted search vectors and
 // the solutions stay FP64.  Once the operator is FP32,
 // the iterated residual drifts from the true one by the FP32 rounding of
 // each product, so at block boundaries, whenever |r| fell by mix_reliable
-// (default 1e-2) since the last check and when the solve stops, the FP64
-// true residual b - (D^dag D + sigma_0) psi_0 replaces it, with the same
-// correction applied to the search vectors (a reliable update); the solve
+// (default 1e-2) since the last check (or, with mix_interval > 0, every
+// mix_interval iterations rounded up to a block) and when the solve stops,
+// the FP64 true residual b - (D^dag D + sigma_0) psi_0 replaces it, with
+// the same correction applied to the search vectors (a reliable update); the solve
 // only ends when the true residual meets the stopping bound.  The FP32
 // products enter only when the residual is small, so the shifted systems,
 // which never see a residual replacement, keep an error of order FP32
@@ -244,7 +245,8 @@ static int ms_run_block(susy_b200_lattice* h, const void* src, void* const* psim
 
   const double fm2 = h->prm.fmass > 1e-8 ? h->prm.fmass * h->prm.fmass : 0.0;
   const int* skip = &h->ms->skip;
-  const int chunk = 2 * MS_BLK;
+  // a fixed reliable-update schedule polls at every block boundary
+  const int chunk = (mixed && h->mix_interval > 0) ? MS_BLK : 2 * MS_BLK;
   double* pd = (double*)(pw + 2);  // pinned: the iterated |r|^2
   bool fp32_op = false;
   double bnorm = 0.0, last_true = 0.0, rsqstop = 0.0;
@@ -254,7 +256,7 @@ static int ms_run_block(susy_b200_lattice* h, const void* src, void* const* psim
     bnorm = last_true = *pd;
     rsqstop = errormin * bnorm;
   }
-  int launched = 0, replacements = 0;
+  int launched = 0, replacements = 0, last_rel = 0;
   std::vector<char> handed(norder, 0);
   // SUSY_B200_CG_TRACE=1 prints the solver's progress at every poll (stderr)
   static const bool trace = [] {
@@ -277,6 +279,35 @@ static int ms_run_block(susy_b200_lattice* h, const void* src, void* const* psim
       if ((k + 1) % MS_BLK == 0) msb_block(h->ms, v, n, s);
     }
   };
+  // Switch to the FP32 operator at iteration it (a block boundary, or the
+  // start); false when a field cannot be allocated
+  auto to_fp32 = [&](int it) -> bool {
+    fp32_op = true;
+    last_rel = it;
+    convert_field(n, p0, 64, p0_32, 32, s);
+    if (h->mix_vec32) {
+      // FP32 residuals from here on (a block boundary, so the residual of
+      // this iteration is the only ring slot the next steps read), and the
+      // operator's input is the FP32 p0 itself.  The shifted search vectors
+      // and the solutions stay FP64: rounding P_j to FP32 every block puts
+      // an error of order u_32 |P_j| (not u_32 |r|) into every shifted
+      // system, which measured 8x the per-shift correction iterations.
+      const int slot = it % (MS_BLK + 1);
+      for (int q = 0; q <= MS_BLK; q++)
+        if (!vec32_field(h, q)) return false;
+      convert_field(n, v.ring[slot], 64, vec32_field(h, slot), 32, s);
+      for (int q = 0; q <= MS_BLK; q++) v.ring[q] = vec32_field(h, q);
+      v.p0 = p0_32;
+      v.f32 = 1;
+    } else {
+      // the operator input from now on: an FP32 copy of p0, kept by the p0
+      // update
+      v.p0_32 = p0_32;
+    }
+    return true;
+  };
+  // fp32_below = 1: the FP32 operator from the first iteration
+  if (mixed && h->mix_switch >= 1.0 && !to_fp32(0)) return set_err(h, SUSY_B200_ENOMEM);
   // A chunk's ~100 launches are captured once per operator precision into a
   // CUDA graph and replayed: every argument of them is fixed for the solve
   // (the convergence test and the freezing of shifts read device state).
@@ -313,30 +344,11 @@ static int ms_run_block(susy_b200_lattice* h, const void* src, void* const* psim
     if (mixed) {
       const double rsq = *pd;
       const int it = pw[1];
+      const bool due = h->mix_interval > 0 ? it - last_rel >= h->mix_interval
+                                            : rsq < h->mix_reliable * h->mix_reliable * last_true;
       if (!fp32_op && !stop && rsq < h->mix_switch * h->mix_switch * bnorm) {
-        fp32_op = true;
-        convert_field(n, p0, 64, p0_32, 32, s);
-        if (h->mix_vec32) {
-          // FP32 residuals from here on (this poll follows a block pass,
-          // so the residual of this iteration is the only ring slot the
-          // next steps read), and the operator's input is the FP32 p0
-          // itself.  The shifted search vectors and the solutions stay
-          // FP64: rounding P_j to FP32 every block puts an error of order
-          // u_32 |P_j| (not u_32 |r|) into every shifted system, which
-          // measured 8x the per-shift correction iterations.
-          const int slot = pw[1] % (MS_BLK + 1);
-          for (int q = 0; q <= MS_BLK; q++)
-            if (!vec32_field(h, q)) return set_err(h, SUSY_B200_ENOMEM);
-          convert_field(n, v.ring[slot], 64, vec32_field(h, slot), 32, s);
-          for (int q = 0; q <= MS_BLK; q++) v.ring[q] = vec32_field(h, q);
-          v.p0 = p0_32;
-          v.f32 = 1;
-        } else {
-          // the operator input from now on: an FP32 copy of p0, kept by the
-          // p0 update
-          v.p0_32 = p0_32;
-        }
-      } else if (fp32_op && (stop || rsq < h->mix_reliable * h->mix_reliable * last_true)) {
+        if (!to_fp32(it)) return set_err(h, SUSY_B200_ENOMEM);
+      } else if (fp32_op && (stop || due)) {
         // reliable update at the block boundary: psi_0 is current
         void* rt64 = refine_field(h, 4, 64);
         if (!rt64) return set_err(h, SUSY_B200_ENOMEM);
@@ -345,6 +357,7 @@ static int ms_run_block(susy_b200_lattice* h, const void* src, void* const* psim
         if (!(rt == rt)) return set_err(h, SUSY_B200_ENAN);
         msb_replace(h->ms, v, n, rt64, rt, s);
         last_true = rt;
+        last_rel = it;
         replacements++;
         stop = (rt <= rsqstop || it >= MaxCG);
       } else if (fp32_op && !(rsq <= 1e4 * last_true)) {

@@ -156,6 +156,8 @@ def load_library(path: str = LIB_PATH):
     L.susy_b200_plaquette.argtypes = [_vp, _dp, _dp]
     L.susy_b200_mixed_params.restype = C.c_int
     L.susy_b200_mixed_params.argtypes = [_vp, C.c_double, C.c_double]
+    L.susy_b200_mixed_reliable_interval.restype = C.c_int
+    L.susy_b200_mixed_reliable_interval.argtypes = [_vp, C.c_int]
     L.susy_b200_mixed_correction.restype = C.c_int
     L.susy_b200_mixed_correction.argtypes = [_vp, C.c_int]
     L.susy_b200_set_solver.restype = C.c_int
@@ -442,6 +444,12 @@ class Lattice:
         residual replacement whenever |r| fell by reliable_factor."""
         self._check(self.lib.susy_b200_mixed_params(self.h, float(fp32_below),
                                                     float(reliable_factor)))
+
+    def mixed_reliable_interval(self, iters: int = 0):
+        """Mixed solver: FP64 residual replacement every iters iterations
+        (rounded up to a block boundary) instead of the reliable_factor
+        trigger; 0 restores the trigger."""
+        self._check(self.lib.susy_b200_mixed_reliable_interval(self.h, int(iters)))
 
     def mixed_correction(self, fp32: bool = True):
         """Mixed solver: per-shift correction solves with the FP32 operator

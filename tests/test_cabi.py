@@ -50,7 +50,8 @@ def test_error_strings_and_null_handles():
     assert lib.susy_b200_fermion_op(None, None, None, 1) == -1
     # solver settings refuse a missing handle before touching the device
     for name, arg in (("susy_b200_pf_streams", 1), ("susy_b200_mixed_correction", 1),
-                      ("susy_b200_use_graphs", 1), ("susy_b200_cg_blocked", 1)):
+                      ("susy_b200_use_graphs", 1), ("susy_b200_cg_blocked", 1),
+                      ("susy_b200_mixed_reliable_interval", 50)):
         f = getattr(lib, name)
         f.restype = C.c_int
         assert f(None, arg) == -1, name

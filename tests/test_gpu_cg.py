@@ -177,6 +177,38 @@ def test_mixed_corrections_meet_bound(fp32):
     assert lat.lib.susy_b200_mixed_correction(lat.h, 2) < 0
 
 
+@pytest.mark.parametrize("interval", [50, 0])
+def test_mixed_fp32_from_start_with_fixed_reliable_updates(interval):
+    """The microbenchmark's literal schedule: the FP32 operator from the
+    first iteration (fp32_below = 1) with the FP64 true residual replacing
+    the iterated one every 50 iterations (rounded up to a block boundary)
+    or on the residual trigger: every shift still ends at the FP64 true
+    residual bound and agrees with the FP64 solver's solution."""
+    dims, N = (8, 8, 8, 8), 2
+    lat = Lattice(dims, N, pbc=-1, lam=1.0, bmass=0.2, G=0.05)
+    lat.set_links(synth.to_ref(dims, synth.links(dims, N, 0.2, 1)))
+    shifts = synth.geometric_shifts(15, 1e-5, 1e3)
+    src = lat.tf(64)
+    src.upload(synth.to_ref(dims, synth.tf_source(dims, N, 62)))
+    b2 = float(np.dot(src.download(), src.download()))
+    ref = [lat.tf(64) for _ in shifts]
+    it64, _ = lat.dev_congrad_multi(src, ref, shifts, 20000, 1e-20, mixed=False)
+    lat.mixed_params(1.0, 1e-2)
+    lat.mixed_reliable_interval(interval)
+    psim = [lat.tf(64) for _ in shifts]
+    it, _ = lat.dev_congrad_multi(src, psim, shifts, 20000, 1e-20, mixed=True)
+    assert it < 3 * it64
+    t = lat.tf(64)
+    for j, s in enumerate(shifts):
+        lat.dev_DSq(psim[j], t)
+        x = psim[j].download()
+        r = src.download() - t.download() - s * x
+        assert float(np.dot(r, r)) <= 1.5e-20 * b2
+        y = ref[j].download()
+        assert np.abs(x - y).max() <= 1e-8 * np.abs(y).max()
+    assert lat.lib.susy_b200_mixed_reliable_interval(lat.h, -1) < 0
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("solver", [0, 1])
 def test_host_congrad_multi_early_copies(solver):
