@@ -735,8 +735,10 @@ def run_batch_case(args):
         lam = float(rng.choice(BATCH_LAMS))
         noise = float(rng.uniform(0.1, 0.3))
         lat = Lattice(dims, 2, pbc=-1, lam=lam, bmass=0.2, G=0.05, iseed=1000 + i)
-        st = torch.cuda.Stream()
-        lat.set_stream(st.cuda_stream)
+        # every lattice keeps its own stream (torch.cuda.Stream() hands out
+        # a pool of 32 per device, so lattices 32 apart would share one);
+        # the events are recorded on it through an ExternalStream
+        st = torch.cuda.ExternalStream(lat.stream)
         links = synth.to_ref(dims, synth.links(dims, 2, noise, 500 + i))
         lats.append(lat)
         streams.append(st)

@@ -64,6 +64,9 @@ int susy_b200_last_error(const susy_b200_lattice *h);
 const char *susy_b200_error_string(int code);
 /* Launch on this cudaStream_t (passed as void*); NULL = the handle's own. */
 int susy_b200_set_stream(susy_b200_lattice *h, void *cuda_stream);
+/* The cudaStream_t (as void*) the handle launches on: its own non-blocking
+ * stream unless susy_b200_set_stream chose another; NULL for a NULL handle. */
+void *susy_b200_get_stream(const susy_b200_lattice *h);
 int susy_b200_sync(susy_b200_lattice *h);
 int susy_b200_volume(const susy_b200_lattice *h);
 /* Number of kernels this library has launched in this process (all handles);
@@ -414,7 +417,11 @@ int susy_b200_dev_congrad_multi_learned(susy_b200_lattice *h, susy_b200_net *net
 /* Independent lattices at once (no reference counterpart: the reference
  * runs one lattice per process): one update() per handle, h[i] with r[i]
  * into res[i], the handles' streams driven concurrently by `threads` host
- * threads (at most n).  Each handle's operator kernels are tuned first, one
+ * threads (at most n).  Every handle must launch on a stream of its own:
+ * two handles on one stream (the same handle twice, or streams set to one
+ * stream by susy_b200_set_stream) return SUSY_B200_EINVAL before any work,
+ * since one thread's graph capture on a stream would take in the other
+ * thread's launches.  Each handle's operator kernels are tuned first, one
  * handle at a time, unless already tuned.  Each lattice's result is the one
  * update() gives it alone.
  * Returns the total CG iterations or the first negative error code. */

@@ -24,6 +24,16 @@ extern "C" int susy_b200_update_batch(susy_b200_lattice* const* hs,
   if (!hs || !rs || !res || n < 0) return SUSY_B200_EINVAL;
   for (int i = 0; i < n; i++)
     if (!hs[i] || !rs[i]) return SUSY_B200_EINVAL;
+  // One stream per handle: a worker captures its solver chunks into CUDA
+  // graphs, and a capture takes in every launch made to its stream, from
+  // any thread, so a second lattice on the same stream would have its work
+  // recorded into the first one's graph and its own syncs refused.
+  {
+    std::vector<cudaStream_t> st(n);
+    for (int i = 0; i < n; i++) st[i] = hs[i]->stream;
+    std::sort(st.begin(), st.end());
+    if (std::adjacent_find(st.begin(), st.end()) != st.end()) return SUSY_B200_EINVAL;
+  }
   // Every handle's operator kernels are tuned here, one handle after the
   // other on this thread with the GPU otherwise idle, before any worker
   // starts: tuned inside the workers, each handle would time its kernels

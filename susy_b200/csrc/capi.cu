@@ -495,6 +495,8 @@ int susy_b200_set_stream(susy_b200_lattice* h, void* s) {
   return SUSY_B200_OK;
 }
 
+void* susy_b200_get_stream(const susy_b200_lattice* h) { return h ? (void*)h->stream : nullptr; }
+
 int susy_b200_sync(susy_b200_lattice* h) {
   if (!h) return SUSY_B200_EINVAL;
   return ck(h, cudaStreamSynchronize(h->stream)) ? SUSY_B200_OK : SUSY_B200_ECUDA;

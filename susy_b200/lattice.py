@@ -125,6 +125,8 @@ def load_library(path: str = LIB_PATH):
     L.susy_b200_error_string.restype = C.c_char_p
     L.susy_b200_error_string.argtypes = [C.c_int]
     L.susy_b200_set_stream.argtypes = [_vp, _vp]
+    L.susy_b200_get_stream.restype = _vp
+    L.susy_b200_get_stream.argtypes = [_vp]
     L.susy_b200_sync.argtypes = [_vp]
     L.susy_b200_volume.argtypes = [_vp]
     L.susy_b200_launch_count.restype = C.c_longlong
@@ -288,6 +290,11 @@ class Lattice:
 
     def set_stream(self, stream_ptr: int | None):
         self._check(self.lib.susy_b200_set_stream(self.h, stream_ptr))
+
+    @property
+    def stream(self) -> int:
+        """The cudaStream_t (as an integer) the lattice launches on."""
+        return int(self.lib.susy_b200_get_stream(self.h) or 0)
 
     def sync(self):
         self._check(self.lib.susy_b200_sync(self.h))

@@ -48,6 +48,7 @@ def test_error_strings_and_null_handles():
     assert lib.susy_b200_error_string(-1) == b"invalid argument"
     assert lib.susy_b200_last_error(None) == -1
     assert lib.susy_b200_fermion_op(None, None, None, 1) == -1
+    assert lib.susy_b200_get_stream(None) is None
     # solver settings refuse a missing handle before touching the device
     for name, arg in (("susy_b200_pf_streams", 1), ("susy_b200_mixed_correction", 1),
                       ("susy_b200_use_graphs", 1), ("susy_b200_cg_blocked", 1),

@@ -13,7 +13,7 @@ import numpy as np
 import pytest
 
 from oracle import susy_np as O
-from susy_b200 import Lattice, RHMC, SOLVER_FP64, SOLVER_MIXED
+from susy_b200 import Lattice, RHMC, SOLVER_FP64, SOLVER_MIXED, SusyError
 from susy_b200 import synth
 from susy_b200.rhmc_tables import rhmc as rhmc_table
 
@@ -326,14 +326,15 @@ def test_update_batch_equals_one_by_one():
 
 
 def test_update_batch_with_more_threads_than_sixteen():
-    """24 lattices on 24 host threads (one per lattice; the pool once had a
-    16-thread cap): every lattice's trajectory is exactly its solo one."""
+    """48 lattices on 48 host threads, each on its own stream (one per
+    lattice; the pool once had a 16-thread cap): every lattice's trajectory
+    is exactly its solo one."""
     from susy_b200 import update_batch
     vols = [(4, 4, 4, 4), (2, 2, 2, 4), (4, 4, 2, 4), (2, 4, 2, 4)]
 
     def build():
         out = []
-        for i in range(24):
+        for i in range(48):
             dims = vols[i % len(vols)]
             lat = Lattice(dims, 2, pbc=-1, lam=[0.5, 1.0, 2.0, 4.0][i % 4], bmass=0.2, G=0.05,
                           iseed=100 + i)
@@ -343,12 +344,38 @@ def test_update_batch_with_more_threads_than_sixteen():
             out.append(lat)
         return out
     rh = [RHMC(15, 1, nstep=2, nstep_gauge=2, traj_length=0.5, error_per_site=1e-6)
-          for _ in range(24)]
-    got = update_batch(build(), rh, threads=24)
+          for _ in range(48)]
+    lats = build()
+    assert len({lat.stream for lat in lats}) == len(lats)
+    got = update_batch(lats, rh, threads=48)
     want = [lat.update(r) for lat, r in zip(build(), rh)]
     for g, w in zip(got, want):
         assert g["accept"] == w["accept"] and g["iters"] == w["iters"]
         assert g["delta_S"] == w["delta_S"] and g["start"] == w["start"]
+
+
+def test_update_batch_refuses_lattices_sharing_a_stream():
+    """Two handles on one stream (a worker's graph capture would take in the
+    other worker's launches): SUSY_B200_EINVAL before any work; on their own
+    streams again, the same batch runs."""
+    from susy_b200 import update_batch
+    dims = (2, 2, 2, 4)
+    lats = []
+    for i in range(2):
+        lat = Lattice(dims, 2, pbc=-1, lam=1.0, bmass=0.2, G=0.05, iseed=300 + i)
+        lat.set_links(synth.to_ref(dims, synth.links(dims, 2, 0.1, 70 + i)))
+        lats.append(lat)
+    rh = [RHMC(15, 1, nstep=2, nstep_gauge=2, traj_length=0.5, error_per_site=1e-6)
+          for _ in lats]
+    own = lats[1].stream
+    lats[1].set_stream(lats[0].stream)
+    with pytest.raises(SusyError):
+        update_batch(lats, rh, threads=2)
+    with pytest.raises(SusyError):
+        update_batch([lats[0], lats[0]], rh, threads=2)
+    lats[1].set_stream(None)
+    assert lats[1].stream == own
+    assert len(update_batch(lats, rh, threads=2)) == 2
 
 
 @pytest.mark.gpu
