@@ -606,10 +606,10 @@ def run_dsq_case(args):
 # Operator and solver microbenchmark: 8^4 U(2), links identity + 0.2
 # noise, lambda 1, bmass 0.2, G 0.05, antiperiodic in time; 32
 # complex-Gaussian sources; 15 shifts geometrically spaced 1e-5 ... 1e3.
-C1_DIMS, C1_NCOL, C1_SOURCES, C1_DSQ = (8, 8, 8, 8), 2, 32, 1000
+MB_DIMS, MB_NCOL, MB_SOURCES, MB_DSQ = (8, 8, 8, 8), 2, 32, 1000
 
 
-def run_config1_case(args):
+def run_microbench_case(args):
     """D^dag D applied 1000 times in FP64 and in FP32, cycling over the 32
     sources (CUDA events on the launching stream; sources and results,
     2 x 32 x 4.2 MB in FP64, exceed the 126 MB L2, the 1.3 MB of links stay
@@ -625,13 +625,13 @@ def run_config1_case(args):
     against the FP64 solver's, max |x - x64| / max |x64|."""
     import torch
     from susy_b200 import Lattice, synth
-    dims, N = C1_DIMS, C1_NCOL
+    dims, N = MB_DIMS, MB_NCOL
     lat = Lattice(dims, N, pbc=-1, lam=1.0, bmass=0.2, G=0.05)
     st = torch.cuda.Stream()
     lat.set_stream(st.cuda_stream)
     lat.set_links(synth.to_ref(dims, synth.links(dims, N, 0.2, 1)))
     peak, peak_kind = measured_peaks()
-    srcs = [synth.to_ref(dims, synth.tf_source(dims, N, 100 + k)) for k in range(C1_SOURCES)]
+    srcs = [synth.to_ref(dims, synth.tf_source(dims, N, 100 + k)) for k in range(MB_SOURCES)]
     a64 = [lat.tf(64) for _ in srcs]
     b64 = [lat.tf(64) for _ in srcs]
     for a, x in zip(a64, srcs):
@@ -641,19 +641,19 @@ def run_config1_case(args):
     for a, c in zip(a64, a32):
         lat.dev_convert(a, c)
     ev = lambda: torch.cuda.Event(enable_timing=True)
-    report = {"case": "config1_microbench", "lattice": "x".join(map(str, dims)), "ncol": N,
-              "sources": len(srcs), "dsq_applications": C1_DSQ, "peak_gbs": peak,
+    report = {"case": "operator_solver_microbench", "lattice": "x".join(map(str, dims)), "ncol": N,
+              "sources": len(srcs), "dsq_applications": MB_DSQ, "peak_gbs": peak,
               "peak_kind": peak_kind}
     for prec, w, A, B in ((64, 16, a64, b64), (32, 8, a32, b32)):
         for k in range(3):
             lat.dev_DSq(A[k], B[k])
         e0, e1 = ev(), ev()
         e0.record(st)
-        for k in range(C1_DSQ):
+        for k in range(MB_DSQ):
             lat.dev_DSq(A[k % len(A)], B[k % len(B)])
         e1.record(st)
         e1.synchronize()
-        ms = e0.elapsed_time(e1) / C1_DSQ
+        ms = e0.elapsed_time(e1) / MB_DSQ
         gbs = 2 * algorithmic_bytes_fop(lat.V, N, w) / (ms * 1e-3) / 1e9
         report["dsq_fp%d" % prec] = {"ms_per_dsq": ms, "algorithmic_gbs": gbs,
                                      "frac": gbs / peak}
@@ -826,6 +826,35 @@ def run_traj_case(args):
                       "runs": out}), flush=True)
 
 
+def run_net_case(args):
+    """The learned network's inference alone (the small case an ncu capture
+    of its kernels runs): 8^4 U(3) (or --dims / --ncol), random weights,
+    three applications to a complex-Gaussian Twist_Fermion, the time of the
+    last two with CUDA events on the lattice's stream."""
+    import torch
+    from susy_b200 import Lattice, synth
+    from susy_b200.learned import Net, init_weights
+    dims = tuple(int(x) for x in args.dims.split(",")) if args.dims else (8, 8, 8, 8)
+    ncol = args.ncol or 3
+    lat = Lattice(dims, ncol, pbc=-1, lam=1.0, bmass=0.2, G=0.05)
+    st = torch.cuda.ExternalStream(lat.stream)
+    lat.set_links(synth.to_ref(dims, synth.links(dims, ncol, 0.2, 3)))
+    net = Net(lat, init_weights(5, scale=0.4))
+    a, b = lat.tf(64), lat.tf(64)
+    a.upload(synth.to_ref(dims, synth.tf_source(dims, ncol, 1)))
+    net.apply(a, b)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    for _ in range(2):
+        net.apply(a, b)
+    e1.record(st)
+    e1.synchronize()
+    print(json.dumps({"case": "net_apply", "lattice": "x".join(map(str, dims)), "ncol": ncol,
+                      "tensor_cores": bool(net.tensor_cores()),
+                      "ms_per_apply": e0.elapsed_time(e1) / 2,
+                      "out_max": float(np.abs(b.download()).max())}), flush=True)
+
+
 def run_learned_case(args):
     """The learned-preconditioner protocol of the benchmark's fourth
     configuration on one lattice (default 8^4 U(2); --dims / --ncol),
@@ -944,7 +973,7 @@ def main():
     ap.add_argument("--variant", type=int, default=-1)
     ap.add_argument("--dims", default="", help="--dsq-case lattice, e.g. 24,24,24,24")
     ap.add_argument("--ncol", type=int, default=0, help="--dsq-case NCOL")
-    ap.add_argument("--config1-case", action="store_true",
+    ap.add_argument("--microbench-case", action="store_true",
                     help="8^4 U(2) operator and solver microbenchmark, 32 sources")
     ap.add_argument("--batch-case", action="store_true",
                     help="independent U(2) lattices of uneven volume, batched vs one by one")
@@ -955,6 +984,8 @@ def main():
     ap.add_argument("--learned-case", action="store_true",
                     help="the learned-preconditioner protocol: chain, pairs, training, "
                          "held-out solves")
+    ap.add_argument("--net-case", action="store_true",
+                    help="the learned network's inference alone, 8^4 U(3)")
     ap.add_argument("--learned-pairs", type=int, default=100)
     ap.add_argument("--learned-steps", type=int, default=300)
     ap.add_argument("--learned-batch", type=int, default=8)
@@ -964,8 +995,8 @@ def main():
     if args.dsq_case:
         run_dsq_case(args)
         return
-    if args.config1_case:
-        run_config1_case(args)
+    if args.microbench_case:
+        run_microbench_case(args)
         return
     if args.batch_case:
         run_batch_case(args)
@@ -975,6 +1006,9 @@ def main():
         return
     if args.learned_case:
         run_learned_case(args)
+        return
+    if args.net_case:
+        run_net_case(args)
         return
 
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -99,7 +99,7 @@ def test_graph_replay_matches_plain_launches(mixed):
         assert np.array_equal(a, b)
 
 
-def test_config1_operator_precisions_and_solvers():
+def test_microbench_operator_precisions_and_solvers():
     """The operator and solver microbenchmark configuration (8^4 U(2),
     links identity + 0.2 noise, lambda 1, bmass 0.2, G 0.05): D^dag D in
     FP64 and FP32 against the FP64 oracle on complex-Gaussian sources, and
