@@ -859,9 +859,8 @@ def run_net_case(args):
 
 
 def run_learned_case(args):
-    """The learned-preconditioner protocol of the benchmark's fourth
-    configuration on one lattice (default 8^4 U(2); --dims / --ncol),
-    lambda 1, bmass 0.2, G 0.05:
+    """The learned-preconditioner protocol on one lattice (default 8^4 U(2);
+    --dims / --ncol), lambda 1, bmass 0.2, G 0.05:
       chain   near-identity links (noise 0.2, seed 31), 200 RHMC
               trajectories (Nroot 1, degree 15, 10 x 2 steps, length 1,
               error_per_site 1e-5), every 5th saved: 40 configurations;
@@ -875,7 +874,8 @@ def run_learned_case(args):
               shift4 poles to the FP64 true residual 1e-10 per site: the
               FP64 multi-shift, the mixed solver, and a multi-shift pass to
               1e-6 followed by flexible CG on the 4 smallest shifts with
-              and without the network (tensor-core inference).
+              and without the network (tensor-core inference); every
+              solve capped at --learned-maxcg (50000) iterations.
     Prints one JSON line per held-out configuration and a summary."""
     import torch
     from susy_b200 import Lattice, RHMC, synth
@@ -934,14 +934,15 @@ def run_learned_case(args):
         b2 = float(np.dot(src.download(), src.download()))
         psim = [lat.tf(64) for _ in shifts]
         row = {"case": "learned_heldout", "config": 30 + c}
-        lat.dev_congrad_multi(src, psim, shifts, 50000, 1e-20)     # warm-up
-        (it, _), ms = timed(lambda: lat.dev_congrad_multi(src, psim, shifts, 50000, 1e-20))
+        cap = args.learned_maxcg
+        lat.dev_congrad_multi(src, psim, shifts, cap, 1e-20)     # warm-up
+        (it, _), ms = timed(lambda: lat.dev_congrad_multi(src, psim, shifts, cap, 1e-20))
         row["fp64"] = {"iterations": it, "ms": ms}
-        (it, _), ms = timed(lambda: lat.dev_congrad_multi(src, psim, shifts, 50000, 1e-20,
+        (it, _), ms = timed(lambda: lat.dev_congrad_multi(src, psim, shifts, cap, 1e-20,
                                                           mixed=True))
         row["mixed"] = {"iterations": it, "ms": ms}
         for name, nn in (("refine_plain", None), ("refine_learned", net)):
-            res, ms = timed(lambda: congrad_multi_learned(lat, nn, src, psim, shifts, 50000,
+            res, ms = timed(lambda: congrad_multi_learned(lat, nn, src, psim, shifts, cap,
                                                            1e-20, nrefine=4, loose=1e-12))
             it, rit, worst = res
             row[name] = {"iterations": it, "refine_iterations": rit, "ms": ms,
@@ -992,6 +993,7 @@ def main():
     ap.add_argument("--learned-pairs", type=int, default=100)
     ap.add_argument("--learned-steps", type=int, default=300)
     ap.add_argument("--learned-batch", type=int, default=8)
+    ap.add_argument("--learned-maxcg", type=int, default=50000)
     ap.add_argument("--lattices", type=int, default=48)
     ap.add_argument("--threads", type=int, default=48)
     args = ap.parse_args()
