@@ -63,3 +63,23 @@ def test_rhmc_degree15_tables():
 def test_geometric_shifts():
     s = synth.geometric_shifts(15, 1e-5, 1e3)
     assert s[0] == pytest.approx(1e-5) and s[-1] == pytest.approx(1e3)
+
+
+def test_reference_arm_assembles_a_solve_from_one_step_of_samples():
+    """bench.py's CPU reference arm: one timed step samples 1, 8 and 15 live
+    shifts; the per-iteration time a + b k is fitted from them and summed
+    over the recorded FP64 schedule, divided by the replicas."""
+    import importlib.util
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    spec = importlib.util.spec_from_file_location("bench_mod", os.path.join(root, "bench.py"))
+    bench = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(bench)
+    arm = bench.CpuArm.__new__(bench.CpuArm)
+    arm.P, arm.kind = 16, "reference"
+    a, b = 2.5, 0.1
+    arm.samples = [(k, a + b * k) for k in bench.REF_SAMPLE_SHIFTS]
+    iters, live_sum, _ = bench.solve_profile()
+    v, desc = arm.value()
+    assert v == pytest.approx((iters * a + b * live_sum) / 16, rel=1e-9)
+    assert "16 single-core replicas" in desc
+    assert len(set(bench.REF_SAMPLE_SHIFTS)) >= 2
