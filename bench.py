@@ -100,6 +100,22 @@ def flops_fop(V, N):
     return 1760 * N ** 3 * V
 
 
+def committed_traffic(v64, v32):
+    """DRAM bytes per operator launch (ncu dram__bytes_read.sum +
+    dram__bytes_write.sum) of the FP64 and FP32 kernel variants the
+    autotuner picked, from the committed single-kernel capture summary
+    profiles/fermion_op_12x12x12x24_u3.json; None for a variant that was
+    never captured (the figure is only quoted for the kernel it measured)."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "fermion_op_12x12x12x24_u3.json")) as f:
+            d = json.load(f)["variants"]
+    except Exception:
+        return None, None
+    t64 = d.get(str(v64), {}).get("fp64_dram_bytes_per_launch")
+    t32 = d.get(str(v32), {}).get("fp32_dram_bytes_per_launch")
+    return t64, t32
+
+
 def measured_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -381,7 +397,13 @@ def run_ours(args, rank, world, device):
     src = lat.tf(64)
     src.upload(src_host)
     psim = [lat.tf(64) for _ in shifts]
-    lat.autotune()
+    if args.fop_variant >= 0:
+        # pinned kernel (e.g. for an ncu launch list, under which the
+        # autotuner's timings are distorted)
+        lat.fop_variant(64, args.fop_variant)
+        lat.fop_variant(32, args.fop_variant)
+    else:
+        lat.autotune()
     mixed = args.solver == "mixed"
 
     def solve(m=None):
@@ -469,12 +491,7 @@ def run_ours(args, rank, world, device):
     algo = algorithmic_bytes_fop(V, NCOL, 16)
     achieved = algo / (fop_ms * 1e-3) / 1e9
     peak, peak_kind = measured_peaks()
-    traffic = None
-    try:
-        with open(os.path.join(ROOT, "profiles", "fermion_op_12x12x12x24_u3.json")) as f:
-            traffic = json.load(f).get("dram_bytes_per_launch")
-    except Exception:
-        pass
+    traffic, traffic32 = committed_traffic(lat.fop_variant(64)[0], lat.fop_variant(32)[0])
 
     # End to end through the public host API: source H2D, every solution D2H
     e2e_ms = None
@@ -534,7 +551,8 @@ def run_ours(args, rank, world, device):
                          "fp32_launch_ms": fop32_ms,
                          "fp32_achieved": algorithmic_bytes_fop(V, NCOL, 8) / (fop32_ms * 1e-3) / 1e9,
                          "fp32_frac": algorithmic_bytes_fop(V, NCOL, 8) / (fop32_ms * 1e-3) / 1e9 / peak,
-                         "fp32_variant": lat.fop_variant(32)[0]},
+                         "fp32_variant": lat.fop_variant(32)[0],
+                         "fp32_traffic": traffic32},
             "clocks": clk.summary(),
             "gpu_launches": launches,
             "e2e": {"value": seconds_per_solve(e2e_ms, args.steps, world) if e2e_ms else None,
@@ -975,6 +993,9 @@ def main():
     ap.add_argument("--dsq-case", action="store_true",
                     help="operator microbenchmark per kernel variant instead of the solve")
     ap.add_argument("--variant", type=int, default=-1)
+    ap.add_argument("--fop-variant", type=int, default=-1,
+                    help="pin the operator kernel variant of the solve in both precisions "
+                         "instead of autotuning it")
     ap.add_argument("--dims", default="", help="--dsq-case lattice, e.g. 24,24,24,24")
     ap.add_argument("--ncol", type=int, default=0, help="--dsq-case NCOL")
     ap.add_argument("--microbench-case", action="store_true",

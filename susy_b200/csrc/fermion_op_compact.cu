@@ -43,6 +43,9 @@ const TermBuilder& fop_terms() {
   return tb;
 }
 
+template <typename R>
+static void prefer_l1_grouped();
+
 static std::mutex g_terms_mu;
 static bool g_terms_ready[64];
 
@@ -81,6 +84,8 @@ int upload_fop_terms(int device, cudaStream_t st) {
   cudaMemcpyToSymbol(c_slot_disp, slot_disp, sizeof(slot_disp));
   cudaMemcpyToSymbol(c_nslot, nslot, sizeof(nslot));
   if (cudaGetLastError() != cudaSuccess) return -2;
+  prefer_l1_grouped<double>();
+  prefer_l1_grouped<float>();
   if (device >= 0 && device < 64) g_terms_ready[device] = true;
   return 0;
 }
@@ -268,17 +273,50 @@ SUSY_D void run_pattern_pp(ACC& acc, const FopArgs<R>& a, int s, unsigned bcm, i
   }
 }
 
+// Longest blocks first.  The site component's blocks cost ~3.5x the others
+// (its determinant epilogue, det_ltos_rt, loads 470 complex numbers against
+// 180 for ten products).  Block b of a grid of 16 blocks per tile over
+// ntile tiles: the ntile site-component blocks first, then the other 15
+// blocks of each tile, tile by tile.  Returns the tile, and k = 0 for the
+// site component, 1..15 for the others.  Measured at 12^3x24 U(3) on one
+// box: the site-major kernel in this order 0.171 ms (FP64) and 0.0996 ms
+// (FP32) per launch against 0.191 and 0.129 with every tile's 16 blocks
+// adjacent (and 0.107 for the component-major FP32 kernel).  The price is
+// DRAM traffic in FP64, whose fields exceed L2: the site-component sweep
+// and the sweep of the other 15 each stream the lattice, 372 MB per launch
+// against 288 MB (264 MB algorithmic); in FP32 141 MB (132 algorithmic).
+// Super-chunks of 48 tiles, each with its site-component blocks first,
+// kept the traffic down but not the time (FP64 0.189 ms).
+SUSY_D int front_block(int b, int ntile, int& k) {
+  if (b < ntile) {
+    k = 0;
+    return b;
+  }
+  b -= ntile;
+  k = 1 + b % 15;
+  return b / 15;
+}
+
 // Block order: site-major (SM = true) or component-major; PP: two operand
 // buffers (prefetch) or one.
 // SHN: the block first copies its output component's neighbour indices
 // (at most MAX_SLOTS displacements x CT_THREADS sites) into shared memory,
 // so a product's operand loads no longer wait on a global index load.
-template <int N, typename R, int SIGN, bool SM, bool PP, int MINB, bool SHN = false>
+// FRONT (with SM): the site component's blocks first, then the others
+// site-major (front_block).
+template <int N, typename R, int SIGN, bool SM, bool PP, int MINB, bool SHN = false,
+          bool FRONT = false>
 __global__ void __launch_bounds__(CT_THREADS, MINB)
 fermion_op_pp_kernel(FopArgs<R> a) {
   if (a.skip && *a.skip) return;
-  const int comp = SM ? blockIdx.x % NTF : blockIdx.x / a.nsb;
-  const int s = (SM ? blockIdx.x / NTF : blockIdx.x % a.nsb) * CT_THREADS + threadIdx.x;
+  int comp, tile;
+  if (FRONT) {
+    tile = front_block(blockIdx.x, a.nsb, comp);
+  } else {
+    comp = SM ? blockIdx.x % NTF : blockIdx.x / a.nsb;
+    tile = SM ? blockIdx.x / NTF : blockIdx.x % a.nsb;
+  }
+  const int s = tile * CT_THREADS + threadIdx.x;
   __shared__ int shn[SHN ? MAX_SLOTS * CT_THREADS : 1];
   if (SHN) {
     const int ns = c_nslot[comp];
@@ -307,6 +345,99 @@ fermion_op_pp_kernel(FopArgs<R> a) {
   }
 }
 
+// Grouped block shape: output components that read the same operands run
+// in one block, one warp each, over the same 32 sites, so an operand one
+// warp fetched is still in the SM's L1 when the next warp of the block asks
+// for it.  Counted over the 160 products, the 15 link and plaquette
+// components read 295 (field, component, displacement) operands per site
+// when each is fetched on its own; in three groups of five -- psi'_0..4,
+// chi'_01..chi'_12, chi'_13..chi'_34 (component order) -- they read 211
+// (e.g. chi_eB(x) is read by both psi'_e and psi'_B, U_e(x - e) by every
+// psi'_B; a search over swaps between groups finds no split into fives
+// that reads fewer).  The site component, whose determinant epilogue
+// (detLtoS) costs ~3.5x its products, runs in blocks of its own (5 warps
+// over 160 sites), so no block waits on one slow warp.  A chunk of 160
+// sites has one site-component block and the 15 group blocks of its five
+// 32-site tiles, in front_block's order.
+// Measured at 12^3x24 U(3) (ncu): the L1 hit rate rises from 6-9% to 30%
+// and the L2 -> L1 traffic falls by 25% (FP64 2.30 -> 1.72 GB, FP32 1.17 ->
+// 0.88 GB per launch), yet the kernel is no faster than the site-major one
+// (FP64 0.205 against 0.171 ms, FP32 0.109 against 0.100): with 15
+// resident warps per SM of which few have a load in flight, the operand
+// gathers are bound by latency, not by L2 bandwidth.  With each chunk's 16
+// blocks adjacent instead, DRAM traffic fell from 365 to 281 MB (FP64) but
+// the kernel took 0.239 / 0.154 ms; blocks of 15 warps (all 15 components,
+// 161 operands per site): 0.224 / 0.117 ms.
+constexpr int GRP_WARPS = 5;
+constexpr int GRP_THREADS = 32 * GRP_WARPS;
+
+template <int N, typename R, int SIGN, int MINB>
+__global__ void __launch_bounds__(GRP_THREADS, MINB)
+fermion_op_grp_kernel(FopArgs<R> a) {
+  if (a.skip && *a.skip) return;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  int k;
+  const int chunk = front_block(blockIdx.x, a.nsb, k);
+  int comp, s;
+  if (k == 0) {
+    comp = 0;
+    s = chunk * GRP_THREADS + threadIdx.x;
+  } else {
+    comp = 1 + ((k - 1) % 3) * GRP_WARPS + warp;
+    s = (chunk * GRP_WARPS + (k - 1) / 3) * 32 + lane;
+  }
+  double part = 0.0;
+  if (s < a.g.V) {
+    const Site c = site_of(a.g, s);
+    const unsigned bcm = bc_mask(a.g, c);
+    AccMat<N, R> acc;
+    acc.zero();
+    run_pattern_pp<N, R, SIGN, P_UF, false>(acc, a, s, bcm, c_pat_start[comp][0], c_pat_start[comp][1]);
+    run_pattern_pp<N, R, SIGN, P_FU, false>(acc, a, s, bcm, c_pat_start[comp][1], c_pat_start[comp][2]);
+    run_pattern_pp<N, R, SIGN, P_FUD, false>(acc, a, s, bcm, c_pat_start[comp][2], c_pat_start[comp][3]);
+    run_pattern_pp<N, R, SIGN, P_UDF, false>(acc, a, s, bcm, c_pat_start[comp][3], c_pat_start[comp][4]);
+    Mat<N, R> out = acc.get();
+    part = fop_finish<N, R, SIGN>(out, a, c, comp);
+  }
+  if (a.dot) {
+    part = block_sum<GRP_THREADS>(part);
+    if (threadIdx.x == 0) a.dot[blockIdx.x] = part;
+  }
+}
+
+// Blocks: 16 per 160-site chunk, 16 ceil(V / 160) in all, within the
+// 16 ceil(V / 32) dot partials fop_partials() sizes.  Resident blocks per
+// SM: 3 in FP64 (at most 136 registers a thread), 6 in FP32 (68).
+template <int N, typename R>
+static int launch_grp(FopArgs<R> a, int sign, cudaStream_t st) {
+  constexpr int MINB = sizeof(R) == 8 ? 3 : 6;
+  a.nsb = (a.g.V + GRP_THREADS - 1) / GRP_THREADS;
+  const int nblk = 16 * a.nsb;
+  if (sign > 0)
+    count_launch(), fermion_op_grp_kernel<N, R, 1, MINB><<<nblk, GRP_THREADS, 0, st>>>(a);
+  else
+    count_launch(), fermion_op_grp_kernel<N, R, -1, MINB><<<nblk, GRP_THREADS, 0, st>>>(a);
+  return nblk;
+}
+
+// The grouped kernels use 40 B of shared memory: ask for the largest L1
+// split, the cache the grouping relies on.  A preference of the current
+// device, set with the term table at lattice creation (outside any stream
+// capture); a refusal only costs speed.
+template <typename R>
+static void prefer_l1_grouped() {
+  constexpr int MINB = sizeof(R) == 8 ? 3 : 6;
+  const void* k[6] = {(const void*)fermion_op_grp_kernel<2, R, 1, MINB>,
+                      (const void*)fermion_op_grp_kernel<2, R, -1, MINB>,
+                      (const void*)fermion_op_grp_kernel<3, R, 1, MINB>,
+                      (const void*)fermion_op_grp_kernel<3, R, -1, MINB>,
+                      (const void*)fermion_op_grp_kernel<4, R, 1, MINB>,
+                      (const void*)fermion_op_grp_kernel<4, R, -1, MINB>};
+  for (const void* f : k)
+    if (cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout, 0) != cudaSuccess)
+      cudaGetLastError();
+}
+
 template <int N, typename R, bool PF>
 static int launch_compact(FopArgs<R> a, int sign, cudaStream_t st) {
   a.nsb = (a.g.V + CT_THREADS - 1) / CT_THREADS;
@@ -318,14 +449,14 @@ static int launch_compact(FopArgs<R> a, int sign, cudaStream_t st) {
   return nblk;
 }
 
-template <int N, typename R, bool SM, bool PP, int MINB = 1, bool SHN = false>
+template <int N, typename R, bool SM, bool PP, int MINB = 1, bool SHN = false, bool FRONT = false>
 static int launch_pp(FopArgs<R> a, int sign, cudaStream_t st) {
   a.nsb = (a.g.V + CT_THREADS - 1) / CT_THREADS;
   const int nblk = a.nsb * NTF;
   if (sign > 0)
-    count_launch(), fermion_op_pp_kernel<N, R, 1, SM, PP, MINB, SHN><<<nblk, CT_THREADS, 0, st>>>(a);
+    count_launch(), fermion_op_pp_kernel<N, R, 1, SM, PP, MINB, SHN, FRONT><<<nblk, CT_THREADS, 0, st>>>(a);
   else
-    count_launch(), fermion_op_pp_kernel<N, R, -1, SM, PP, MINB, SHN><<<nblk, CT_THREADS, 0, st>>>(a);
+    count_launch(), fermion_op_pp_kernel<N, R, -1, SM, PP, MINB, SHN, FRONT><<<nblk, CT_THREADS, 0, st>>>(a);
   return nblk;
 }
 
@@ -376,6 +507,20 @@ int fermion_op_compact(const FopArgs<R>& a, int N, int sign, int variant, cudaSt
         case 2: return launch_pp<2, R, false, false, 8, true>(a, sign, st);
         case 3: return launch_pp<3, R, false, false, 8, true>(a, sign, st);
         default: return launch_pp<4, R, false, false, 8, true>(a, sign, st);
+      }
+    case FOP_SITE_MAJOR_FRONT: {
+      constexpr int MB = sizeof(R) == 8 ? 4 : 8;
+      switch (N) {
+        case 2: return launch_pp<2, R, true, false, MB, false, true>(a, sign, st);
+        case 3: return launch_pp<3, R, true, false, MB, false, true>(a, sign, st);
+        default: return launch_pp<4, R, true, false, MB, false, true>(a, sign, st);
+      }
+    }
+    case FOP_GROUPED:
+      switch (N) {
+        case 2: return launch_grp<2, R>(a, sign, st);
+        case 3: return launch_grp<3, R>(a, sign, st);
+        default: return launch_grp<4, R>(a, sign, st);
       }
     default:
       switch (N) {

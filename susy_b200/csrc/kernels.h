@@ -87,10 +87,16 @@ struct MsBlockVecs {
 // the 64-register component-major kernel (0.117 ms vs 0.135; 48: 0.166).
 // FOP_SITE_MAJOR_SHN / FOP_COMP_MAJOR_SHN: the _OCC kernels with each
 // block's neighbour indices preloaded into shared memory.
+// FOP_SITE_MAJOR_FRONT: site-major (FP64 4, FP32 8 blocks per SM) with the
+// site component's long blocks at the front of the grid.
+// FOP_GROUPED: one output component per warp over the same 32 sites, the
+// components in groups of five that share operands (fermion_op_compact.cu;
+// 3 resident blocks of 5 warps per SM in FP64, 6 in FP32).
 enum { FOP_MAT = 0, FOP_MAT_CM = 1, FOP_ROWS = 2, FOP_COMPACT = 3, FOP_COMPACT_PF = 4,
        FOP_SITE_MAJOR_PP = 5, FOP_COMP_MAJOR_PP = 6, FOP_SITE_MAJOR = 7,
        FOP_SITE_MAJOR_OCC = 8, FOP_COMP_MAJOR_OCC = 9, FOP_SITE_MAJOR_SHN = 10,
-       FOP_COMP_MAJOR_SHN = 11, FOP_NVARIANTS = 12 };
+       FOP_COMP_MAJOR_SHN = 11, FOP_SITE_MAJOR_FRONT = 12, FOP_GROUPED = 13,
+       FOP_NVARIANTS = 14 };
 template <typename R>
 int fermion_op(const Geo& g, int N, const void* U, const void* Uinv, const void* pd,
                 const void* src, void* dst, int sign, double G, const void* add, double addc,
