@@ -229,7 +229,7 @@ int susy_b200_set_rescale(susy_b200_lattice *h, int on);
  * counterpart in the reference.
  * fp32 < 0 only queries; returns the previous setting. */
 int susy_b200_mixed_vectors(susy_b200_lattice *h, int fp32);
-#define SUSY_B200_FOP_NVARIANTS 14   /* entries of ms_per_variant */
+#define SUSY_B200_FOP_NVARIANTS 15   /* entries of ms_per_variant */
 int susy_b200_autotune(susy_b200_lattice *h);
 int susy_b200_fop_variant(susy_b200_lattice *h, int prec, int set_to, float *ms_per_variant);
 int susy_b200_dev_DSq(susy_b200_lattice *h, const void *src, void *dst, int prec);

@@ -131,9 +131,9 @@ static int launch_variant(susy_b200_lattice* h, const void* src, void* dst, int 
   if (h->rescale && v < FOP_COMPACT) v = FOP_SITE_MAJOR_OCC;
   if (prec == 64)
     return fermion_op<double>(h->g, h->N, h->U, h->Uinv, h->pd, src, dst, sign, h->G, add, addc,
-                              dot, skip, v, h->nbrtab, h->stream, es);
+                              dot, skip, v, h->nbrtab, h->stream, es, h->trace[0]);
   return fermion_op<float>(h->g, h->N, h->U32, h->Uinv32, h->pd32, src, dst, sign, h->G, add,
-                           addc, dot, skip, v, h->nbrtab, h->stream, es);
+                           addc, dot, skip, v, h->nbrtab, h->stream, es, h->trace[1]);
 }
 
 // Project-written autotuner: time one D^dag D with every kernel variant on
@@ -236,7 +236,9 @@ susy_b200_lattice* solver_shadow(susy_b200_lattice* h) {
     }
     c->stream = c->own_stream;
     c->ms = (MsState*)dalloc(c, sizeof(MsState));
-    if (!c->ms) {
+    c->trace[0] = dalloc(c, 5 * c->g.S * sizeof(double2));
+    c->trace[1] = dalloc(c, 5 * c->g.S * sizeof(float2));
+    if (!c->ms || !c->trace[0] || !c->trace[1]) {
       susy_b200_destroy(c);
       return nullptr;
     }
@@ -313,6 +315,8 @@ susy_b200_lattice* susy_b200_create(const susy_b200_params* p) {
   h->stage = dalloc(h, (size_t)h->g.V * NTF * mat_c(h) * 2 * sizeof(double));
   h->ms = (MsState*)dalloc(h, sizeof(MsState));
   h->nbrtab = (int*)dalloc(h, (size_t)fop_ndisp() * h->g.S * sizeof(int));
+  h->trace[0] = dalloc(h, 5 * h->g.S * sizeof(double2));
+  h->trace[1] = dalloc(h, 5 * h->g.S * sizeof(float2));
   if (h->nbrtab) build_nbr_table(h->g, h->nbrtab, h->stream);
   if (h->err) {
     susy_b200_destroy(h);
@@ -342,7 +346,7 @@ void susy_b200_destroy(susy_b200_lattice* h) {
     h->U = h->Uinv = h->pd = h->U32 = h->Uinv32 = h->pd32 = nullptr, h->nbrtab = nullptr;
   void* ptrs[] = {h->U, h->mom, h->Uinv, h->force, h->det, h->pd, h->zw, h->D, h->F,
                   h->U32, h->Uinv32, h->pd32, h->stage, h->ms, h->bigpart, h->gen, h->prn,
-                  h->rng_bad, h->ptrbuf, h->nbrtab, h->meas};
+                  h->rng_bad, h->ptrbuf, h->nbrtab, h->meas, h->trace[0], h->trace[1]};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (int i = 0; i < SUSY_NSCRATCH; i++) {

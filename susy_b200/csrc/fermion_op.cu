@@ -259,7 +259,7 @@ template <typename R>
 int fermion_op(const Geo& g, int N, const void* U, const void* Uinv, const void* pd,
                 const void* src, void* dst, int sign, double G, const void* add,
                 double addc, double* dot, const int* skip, int variant, const int* nbrtab,
-                cudaStream_t st, double eta_scale) {
+                cudaStream_t st, double eta_scale, void* trace) {
   typedef typename CT<R>::T T;
   FopArgs<R> a;
   a.g = g;
@@ -276,6 +276,8 @@ int fermion_op(const Geo& g, int N, const void* U, const void* Uinv, const void*
   a.skip = skip;
   a.nbrtab = nbrtab;
   a.eta_scale = (R)eta_scale;
+  a.trace = (T*)trace;
+  if (variant == FOP_SITE_MAJOR_TR && !trace) variant = FOP_SITE_MAJOR_FRONT;
   if (variant == FOP_ROWS) return fermion_op_rows<R>(a, N, sign, st);
   if (variant >= FOP_COMPACT) return fermion_op_compact<R>(a, N, sign, variant, st);
   a.comp_major = variant == FOP_MAT_CM;
@@ -288,9 +290,11 @@ int fermion_op(const Geo& g, int N, const void* U, const void* Uinv, const void*
 
 template int fermion_op<double>(const Geo&, int, const void*, const void*, const void*,
                                  const void*, void*, int, double, const void*, double,
-                                 double*, const int*, int, const int*, cudaStream_t, double);
+                                 double*, const int*, int, const int*, cudaStream_t, double,
+                                 void*);
 template int fermion_op<float>(const Geo&, int, const void*, const void*, const void*,
                                 const void*, void*, int, double, const void*, double,
-                                double*, const int*, int, const int*, cudaStream_t, double);
+                                double*, const int*, int, const int*, cudaStream_t, double,
+                                void*);
 
 }  // namespace susy

@@ -303,9 +303,9 @@ SUSY_D int front_block(int b, int ntile, int& k) {
 // (at most MAX_SLOTS displacements x CT_THREADS sites) into shared memory,
 // so a product's operand loads no longer wait on a global index load.
 // FRONT (with SM): the site component's blocks first, then the others
-// site-major (front_block).
+// site-major (front_block).  TR: detLtoS from the pre-pass's traces.
 template <int N, typename R, int SIGN, bool SM, bool PP, int MINB, bool SHN = false,
-          bool FRONT = false>
+          bool FRONT = false, bool TR = false>
 __global__ void __launch_bounds__(CT_THREADS, MINB)
 fermion_op_pp_kernel(FopArgs<R> a) {
   if (a.skip && *a.skip) return;
@@ -337,7 +337,7 @@ fermion_op_pp_kernel(FopArgs<R> a) {
     run_pattern_pp<N, R, SIGN, P_FUD, PP>(acc, a, s, bcm, c_pat_start[comp][2], c_pat_start[comp][3], sh);
     run_pattern_pp<N, R, SIGN, P_UDF, PP>(acc, a, s, bcm, c_pat_start[comp][3], c_pat_start[comp][4], sh);
     Mat<N, R> out = acc.get();
-    part = fop_finish<N, R, SIGN>(out, a, c, comp);
+    part = fop_finish<N, R, SIGN, TR>(out, a, c, comp);
   }
   if (a.dot) {
     part = block_sum<CT_THREADS>(part);
@@ -449,14 +449,22 @@ static int launch_compact(FopArgs<R> a, int sign, cudaStream_t st) {
   return nblk;
 }
 
-template <int N, typename R, bool SM, bool PP, int MINB = 1, bool SHN = false, bool FRONT = false>
+template <int N, typename R, bool SM, bool PP, int MINB = 1, bool SHN = false, bool FRONT = false,
+          bool TR = false>
 static int launch_pp(FopArgs<R> a, int sign, cudaStream_t st) {
   a.nsb = (a.g.V + CT_THREADS - 1) / CT_THREADS;
   const int nblk = a.nsb * NTF;
+  if (TR && a.doG) {   // the traces detLtoS reads, for this sign's source
+    const dim3 nb((a.g.V + CT_THREADS - 1) / CT_THREADS, NUMLINK);
+    if (sign > 0)
+      count_launch(), k_det_traces<N, R, false><<<nb, CT_THREADS, 0, st>>>(a);
+    else
+      count_launch(), k_det_traces<N, R, true><<<nb, CT_THREADS, 0, st>>>(a);
+  }
   if (sign > 0)
-    count_launch(), fermion_op_pp_kernel<N, R, 1, SM, PP, MINB, SHN, FRONT><<<nblk, CT_THREADS, 0, st>>>(a);
+    count_launch(), fermion_op_pp_kernel<N, R, 1, SM, PP, MINB, SHN, FRONT, TR><<<nblk, CT_THREADS, 0, st>>>(a);
   else
-    count_launch(), fermion_op_pp_kernel<N, R, -1, SM, PP, MINB, SHN, FRONT><<<nblk, CT_THREADS, 0, st>>>(a);
+    count_launch(), fermion_op_pp_kernel<N, R, -1, SM, PP, MINB, SHN, FRONT, TR><<<nblk, CT_THREADS, 0, st>>>(a);
   return nblk;
 }
 
@@ -514,6 +522,14 @@ int fermion_op_compact(const FopArgs<R>& a, int N, int sign, int variant, cudaSt
         case 2: return launch_pp<2, R, true, false, MB, false, true>(a, sign, st);
         case 3: return launch_pp<3, R, true, false, MB, false, true>(a, sign, st);
         default: return launch_pp<4, R, true, false, MB, false, true>(a, sign, st);
+      }
+    }
+    case FOP_SITE_MAJOR_TR: {
+      constexpr int MB = sizeof(R) == 8 ? 4 : 8;
+      switch (N) {
+        case 2: return launch_pp<2, R, true, false, MB, false, true, true>(a, sign, st);
+        case 3: return launch_pp<3, R, true, false, MB, false, true, true>(a, sign, st);
+        default: return launch_pp<4, R, true, false, MB, false, true, true>(a, sign, st);
       }
     }
     case FOP_GROUPED:

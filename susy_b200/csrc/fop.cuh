@@ -24,6 +24,8 @@ struct FopArgs {
   const int* nbrtab;  // neighbour index table of the table-driven variant
   R eta_scale;        // 2 with the reference's RESCALE (the site component of
                       // input and output doubled, utilities.c:795,841), else 1
+  T* trace;           // FOP_SITE_MAJOR_TR: the five traces Tr(U_e^-1 src_{1+e})
+                      // of every site, [e][S] (written by its pre-pass)
 };
 
 constexpr int FOP_THREADS = 128;

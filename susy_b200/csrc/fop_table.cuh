@@ -226,6 +226,52 @@ SUSY_D void det_ltos_rt(Mat<N, R>& acc, const FopArgs<R>& a, const Site& c) {
   for (int i = 0; i < N; i++) acc.e[i][i] = acc.e[i][i] + d;
 }
 
+// Every site's five detLtoS traces Tr(U_e^-1(x) src_{1+e}(x)) (the source
+// adjointed for D^dag), tr[e * S + x], summed as trace_ld sums them: the
+// pre-pass of FOP_SITE_MAJOR_TR.  One thread per (site, e), e = blockIdx.y:
+// one thread per site looping over e left too few loads in flight (the
+// pre-pass took ~25 us in FP64 at 12^3x24 U(3), for 63 MB; now 11.5 us).
+// Measured there (ncu, FP64): the operator kernel after it takes 147-154 us
+// against 167-176 us recomputing the traces, moves 2.01 against 2.30 GB
+// from L2 and 319 against 372 MB of DRAM (the site component's blocks no
+// longer gather 470 complex numbers each); pre-pass included, D^dag D runs
+// at 0.169 / 0.098 ms per launch (FP64 / FP32) against 0.170 / 0.099
+// without it, and 0.171 / 0.101 with the trace pre-pass but the plain
+// site-major block order.
+template <int N, typename R, bool ADJ>
+__global__ void k_det_traces(FopArgs<R> a) {
+  if (a.skip && *a.skip) return;
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  const int e = blockIdx.y;
+  if (s >= a.g.V) return;
+  const int S = a.g.S;
+  stc<R>(a.trace + (size_t)e * S + s, trace_ld<N, R, ADJ>(a.Uinv, e, s, a.src, 1 + e, s, S));
+}
+
+// detLtoS from the pre-pass's traces: the sums of det_ltos_rt in the same
+// order, 25 trace loads in place of 25 traces of two matrices each
+template <int N, typename R, int SIGN>
+SUSY_D void det_ltos_tr(Mat<N, R>& acc, const FopArgs<R>& a, const Site& c) {
+  const Geo& g = a.g;
+  const int S = g.S, s = c.s;
+  Cx<R> tsum(0, 0);
+#pragma unroll 1
+  for (int b = 0; b < NUMLINK; b++) {
+    const int pb = nbr(g, c, ex(b), ey(b), ez(b), et(b));
+    const R bcb = bcf<R>(g, c, et(b));
+    const Cx<R> T0b = ldc<R>(a.trace + (size_t)b * S + s);
+#pragma unroll 1
+    for (int e = 0; e < NUMLINK; e++) {
+      if (e == b) continue;
+      const Cx<R> Tp = ldc<R>(a.trace + (size_t)e * S + pb);
+      tsum = tsum + ldc<R>(a.pd + (size_t)(e * 5 + b) * S + s) * (T0b + bcb * Tp);
+    }
+  }
+  const Cx<R> d = ((R)0.5 * a.G) * tsum;
+#pragma unroll
+  for (int i = 0; i < N; i++) acc.e[i][i] = acc.e[i][i] + d;
+}
+
 // The reference's RESCALE doubles the site component of the output
 // (utilities.c:841-844)
 template <int N, typename R>
@@ -238,13 +284,18 @@ SUSY_D void eta_rescale(Mat<N, R>& acc, R sc) {
 }
 
 // Shared epilogue: determinant terms, adjoint for D^dag, axpy and dot
-template <int N, typename R, int SIGN>
+// (TR: detLtoS from the traces of k_det_traces)
+template <int N, typename R, int SIGN, bool TR = false>
 SUSY_D double fop_finish(Mat<N, R>& acc, const FopArgs<R>& a, const Site& c, int comp) {
   if (a.doG) {
-    if (comp == 0)
-      det_ltos_rt<N, R, SIGN>(acc, a, c);
-    else if (comp <= NUMLINK)
+    if (comp == 0) {
+      if (TR)
+        det_ltos_tr<N, R, SIGN>(acc, a, c);
+      else
+        det_ltos_rt<N, R, SIGN>(acc, a, c);
+    } else if (comp <= NUMLINK) {
       det_stol_rt<N, R, SIGN>(acc, a, c, comp - 1);
+    }
   }
   if (comp == 0) eta_rescale(acc, a.eta_scale);
   if (SIGN < 0) {

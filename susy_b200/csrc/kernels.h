@@ -92,16 +92,22 @@ struct MsBlockVecs {
 // FOP_GROUPED: one output component per warp over the same 32 sites, the
 // components in groups of five that share operands (fermion_op_compact.cu;
 // 3 resident blocks of 5 warps per SM in FP64, 6 in FP32).
+// FOP_SITE_MAJOR_TR: FOP_SITE_MAJOR_FRONT after a pre-pass that writes
+// every site's five determinant traces, which the site component's detLtoS
+// term then reads instead of recomputing them at the site and its
+// neighbours (needs the handle's 5 S complex trace field; without one it
+// runs as FOP_SITE_MAJOR_FRONT).  The autotuner's pick in both precisions at
+// 12^3x24 U(3).
 enum { FOP_MAT = 0, FOP_MAT_CM = 1, FOP_ROWS = 2, FOP_COMPACT = 3, FOP_COMPACT_PF = 4,
        FOP_SITE_MAJOR_PP = 5, FOP_COMP_MAJOR_PP = 6, FOP_SITE_MAJOR = 7,
        FOP_SITE_MAJOR_OCC = 8, FOP_COMP_MAJOR_OCC = 9, FOP_SITE_MAJOR_SHN = 10,
        FOP_COMP_MAJOR_SHN = 11, FOP_SITE_MAJOR_FRONT = 12, FOP_GROUPED = 13,
-       FOP_NVARIANTS = 14 };
+       FOP_SITE_MAJOR_TR = 14, FOP_NVARIANTS = 15 };
 template <typename R>
 int fermion_op(const Geo& g, int N, const void* U, const void* Uinv, const void* pd,
                 const void* src, void* dst, int sign, double G, const void* add, double addc,
                 double* dot, const int* skip, int variant, const int* nbrtab, cudaStream_t st,
-                double eta_scale = 1.0);
+                double eta_scale = 1.0, void* trace = nullptr);
 template <typename R> struct FopArgs;
 template <typename R>
 int fermion_op_rows(const FopArgs<R>& a, int N, int sign, cudaStream_t st);

@@ -28,6 +28,8 @@ struct susy_b200_lattice {
   void *U32 = nullptr, *Uinv32 = nullptr, *pd32 = nullptr;
   void* stage = nullptr;  // AoS staging buffer (one FP64 Twist_Fermion)
   int* nbrtab = nullptr;  // neighbour index table of the table-driven operator
+  void* trace[2] = {};    // determinant traces of FOP_SITE_MAJOR_TR (FP64, FP32);
+                          // each solver context owns its own
   susy::MsState* ms = nullptr;
   void* tf64[SUSY_NSCRATCH] = {};
   void* tf32[SUSY_NSCRATCH] = {};

@@ -48,7 +48,7 @@ SOLVER_FP64 = 0
 SOLVER_MIXED = 1
 HMC = 0
 SMD = 1
-FOP_NVARIANTS = 14
+FOP_NVARIANTS = 15
 
 
 class Meas(C.Structure):
