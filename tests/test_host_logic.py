@@ -83,3 +83,38 @@ def test_reference_arm_assembles_a_solve_from_one_step_of_samples():
     assert v == pytest.approx((iters * a + b * live_sum) / 16, rel=1e-9)
     assert "16 single-core replicas" in desc
     assert len(set(bench.REF_SAMPLE_SHIFTS)) >= 2
+
+
+def _bench_module():
+    import importlib.util
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    spec = importlib.util.spec_from_file_location("bench_mod", os.path.join(root, "bench.py"))
+    bench = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(bench)
+    return bench
+
+
+def test_operator_variant_count_agrees_across_header_binding_and_kernels():
+    """ms_per_variant arrays are sized by SUSY_B200_FOP_NVARIANTS: the C
+    header, the ctypes binding and the kernels' variant enum must agree."""
+    import re
+    from susy_b200.lattice import FOP_NVARIANTS
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    hdr = open(os.path.join(root, "include", "susy_b200.h")).read()
+    kern = open(os.path.join(root, "susy_b200", "csrc", "kernels.h")).read()
+    n_hdr = int(re.search(r"#define SUSY_B200_FOP_NVARIANTS (\d+)", hdr).group(1))
+    n_enum = int(re.search(r"FOP_NVARIANTS = (\d+)", kern).group(1))
+    assert n_hdr == n_enum == FOP_NVARIANTS
+
+
+def test_bench_quotes_ncu_traffic_only_for_captured_variants():
+    """roofline.traffic comes from the committed single-kernel capture of
+    the variant the autotuner picked, and is None for one never captured."""
+    bench = _bench_module()
+    t64, t32 = bench.committed_traffic(14, 14)
+    alg64 = bench.algorithmic_bytes_fop(12 * 12 * 12 * 24, 3, 16)
+    alg32 = bench.algorithmic_bytes_fop(12 * 12 * 12 * 24, 3, 8)
+    assert alg64 == 264093696 and alg32 == 132046848
+    # DRAM traffic of a real capture: near the algorithmic bytes, not far below
+    assert 0.9 * alg64 < t64 < 2.0 * alg64 and 0.9 * alg32 < t32 < 2.0 * alg32
+    assert bench.committed_traffic(0, 1) == (None, None)
