@@ -741,6 +741,81 @@ BATCH_VOLS = [(4, 4, 4, 4), (6, 6, 6, 6), (8, 8, 8, 8), (4, 4, 4, 8), (6, 6, 6, 
 BATCH_LAMS = [0.5, 1.0, 2.0, 4.0]
 
 
+def run_batch_dsq_case(args):
+    """D^dag D on --lattices independent U(2) lattices (the batched scan's
+    volumes, lambdas and link noise), FP64 and FP32: all lattices in one
+    pair of persistent launches over a work table (susy_b200_DSq_batch)
+    against each lattice's own D^dag D in turn on one stream (two launches
+    per lattice, the autotuned variant).  Device time with CUDA events, 3
+    warm-up and 20 timed repetitions; site-applications/s = sum of volumes /
+    time per repetition, and the largest relative difference between the
+    batched and the per-lattice results.  Every lattice launches on one
+    stream here, so both ways are timed by the same events."""
+    import torch
+    from susy_b200 import Lattice, dsq_batch, synth
+    rng = np.random.default_rng(2024)
+    lats = []
+    for i in range(args.lattices):
+        dims = BATCH_VOLS[int(rng.integers(len(BATCH_VOLS)))]
+        lam = float(rng.choice(BATCH_LAMS))
+        noise = float(rng.uniform(0.1, 0.3))
+        lat = Lattice(dims, 2, pbc=-1, lam=lam, bmass=0.2, G=0.05, iseed=1000 + i)
+        lat.set_links(synth.to_ref(dims, synth.links(dims, 2, noise, 500 + i)))
+        lat.autotune()
+        lats.append(lat)
+    sites = sum(lat.V for lat in lats)
+    # both ways on one stream, so the events on it see every launch
+    torch.cuda.synchronize()
+    st = torch.cuda.Stream()
+    for lat in lats:
+        lat.set_stream(st.cuda_stream)
+    for prec in (64, 32):
+        srcs, outs, refs = [], [], []
+        for i, lat in enumerate(lats):
+            s64 = lat.tf(64)
+            s64.upload(synth.to_ref(lat.dims, synth.tf_source(lat.dims, 2, 700 + i)))
+            if prec == 64:
+                s = s64
+            else:
+                s = lat.tf(32)
+                lat.dev_convert(s64, s)
+            srcs.append(s)
+            outs.append(lat.tf(prec))
+            refs.append(lat.tf(prec))
+        torch.cuda.synchronize()
+
+        def one_by_one():
+            for lat, s, r in zip(lats, srcs, refs):
+                lat.dev_DSq(s, r)
+
+        def batched():
+            dsq_batch(srcs, outs, st.cuda_stream)
+
+        res = {}
+        for name, fn in (("batched", batched), ("one_by_one", one_by_one)):
+            for _ in range(3):
+                fn()
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            for _ in range(20):
+                fn()
+            e1.record(st)
+            torch.cuda.synchronize()
+            res[name] = e0.elapsed_time(e1) / 20
+        err = max(float(np.abs(o.download() - r.download()).max() /
+                        np.abs(r.download()).max()) for o, r in zip(outs, refs))
+        print(json.dumps({"case": "dsq_batch", "lattices": len(lats), "sites": sites,
+                          "prec": prec, "ms_batched": res["batched"],
+                          "ms_one_by_one": res["one_by_one"],
+                          "site_applications_per_s_batched": sites / (res["batched"] * 1e-3),
+                          "site_applications_per_s_one_by_one":
+                              sites / (res["one_by_one"] * 1e-3),
+                          "speedup": res["one_by_one"] / res["batched"],
+                          "max_rel_diff": err}), flush=True)
+
+
 def run_batch_case(args):
     """One RHMC trajectory on each of --lattices independent lattices,
     concurrently (susy_b200_update_batch) and one after another, from the
@@ -1002,6 +1077,8 @@ def main():
                     help="8^4 U(2) operator and solver microbenchmark, 32 sources")
     ap.add_argument("--batch-case", action="store_true",
                     help="independent U(2) lattices of uneven volume, batched vs one by one")
+    ap.add_argument("--batch-dsq-case", action="store_true",
+                    help="D^dag D on the independent lattices in one launch vs one by one")
     ap.add_argument("--traj-solvers", default="",
                     help="with --traj-case: comma list of mixed, mixed_fp64_corrections, fp64")
     ap.add_argument("--traj-case", action="store_true",
@@ -1026,6 +1103,9 @@ def main():
         return
     if args.batch_case:
         run_batch_case(args)
+        return
+    if args.batch_dsq_case:
+        run_batch_dsq_case(args)
         return
     if args.traj_case:
         run_traj_case(args)

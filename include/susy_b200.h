@@ -428,6 +428,23 @@ int susy_b200_dev_congrad_multi_learned(susy_b200_lattice *h, susy_b200_net *net
 int susy_b200_update_batch(susy_b200_lattice *const *h, const susy_b200_rhmc *const *r,
                            susy_b200_traj *res, int n, int threads);
 
+/* dst[i] = (D^dag D + fmass_i^2) src[i] on lattice h[i], for n independent
+ * lattices in two persistent launches over one work table of (lattice,
+ * 128-site tile, output component) items instead of two launches per
+ * lattice (no reference counterpart: the reference applies DSq,
+ * utilities.c:874, to one lattice per process).  1 <= n <= 64 handles of
+ * one NCOL on one device; lattice sizes, couplings and the RESCALE setting
+ * may differ.  src[i] and dst[i] are device fields of h[i] in precision
+ * prec (64 or 32).  Launches on cuda_stream (NULL: h[0]'s stream), after
+ * the work already queued on every handle's stream, which in turn waits
+ * for the launches, so the call is ordered like each handle's own
+ * susy_b200_dev_DSq.  Each lattice's result is the one the site-major
+ * table-driven kernels give it alone.  Uses (and on first use allocates)
+ * each handle's DSq scratch field. */
+#define SUSY_B200_BATCH_MAX 64
+int susy_b200_DSq_batch(susy_b200_lattice *const *h, const void *const *src, void *const *dst,
+                        int n, int prec, void *cuda_stream);
+
 #ifdef __cplusplus
 }
 #endif

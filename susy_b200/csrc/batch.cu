@@ -9,6 +9,7 @@
 #include <atomic>
 #include <thread>
 #include <vector>
+#include "fop.cuh"
 #include "lattice.h"
 
 namespace susy {
@@ -68,4 +69,103 @@ extern "C" int susy_b200_update_batch(susy_b200_lattice* const* hs,
     total += res[i].iters;
   }
   return (int)std::min<long long>(total, 0x7fffffff);
+}
+
+// D^dag D (+ fmass^2) on device fields of many lattices in two launches
+// (fermion_op_batch): the D of every lattice, then the D^dag of every
+// lattice with the fmass^2 term.  Each lattice's intermediate field is its
+// handle's DSq scratch field (allocated on the handle's first DSq).  The
+// launches go to one stream, ordered after the work already queued on every
+// handle's stream, and every handle's stream is ordered after them (events),
+// so the call behaves like each handle's own DSq on its own stream.
+template <typename R>
+static FopArgs<R> batch_args(susy_b200_lattice* h, const void* src, void* dst, const void* add,
+                             double addc) {
+  typedef typename CT<R>::T T;
+  const bool f64 = sizeof(R) == 8;
+  FopArgs<R> a;
+  a.g = h->g;
+  a.U = (const T*)(f64 ? h->U : h->U32);
+  a.Uinv = (const T*)(f64 ? h->Uinv : h->Uinv32);
+  a.pd = (const T*)(f64 ? h->pd : h->pd32);
+  a.src = (const T*)src;
+  a.dst = (T*)dst;
+  a.G = (R)h->G;
+  a.doG = h->G > 1e-8;
+  a.add = (const T*)add;
+  a.addc = (R)addc;
+  a.dot = nullptr;
+  a.skip = nullptr;
+  a.comp_major = 0;
+  a.nsb = 0;
+  a.nbrtab = h->nbrtab;
+  a.eta_scale = (R)(h->rescale ? 2.0 : 1.0);
+  a.trace = nullptr;
+  return a;
+}
+
+template <typename R>
+static int dsq_batch(susy_b200_lattice* const* hs, const void* const* src, void* const* dst,
+                     int n, cudaStream_t st) {
+  const int prec = sizeof(R) == 8 ? 64 : 32;
+  std::vector<void*> tmp(n);
+  for (int i = 0; i < n; i++)
+    if (!(tmp[i] = scratch_tf(hs[i], 0, prec))) return SUSY_B200_ENOMEM;
+  int dev = 0, sms = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+    cudaGetLastError();
+    return SUSY_B200_ECUDA;
+  }
+  std::vector<cudaStream_t> others;
+  for (int i = 0; i < n; i++)
+    if (hs[i]->stream != st &&
+        std::find(others.begin(), others.end(), hs[i]->stream) == others.end())
+      others.push_back(hs[i]->stream);
+  auto order = [](cudaStream_t from, cudaStream_t to) -> bool {
+    cudaEvent_t e;
+    if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) return false;
+    const bool ok = cudaEventRecord(e, from) == cudaSuccess && cudaStreamWaitEvent(to, e, 0) == cudaSuccess;
+    cudaEventDestroy(e);   // released once the recorded work completes
+    return ok;
+  };
+  for (cudaStream_t o : others)
+    if (!order(o, st)) {
+      cudaGetLastError();
+      return SUSY_B200_ECUDA;
+    }
+  std::vector<FopArgs<R>> a(n);
+  for (int i = 0; i < n; i++) a[i] = batch_args<R>(hs[i], src[i], tmp[i], nullptr, 0.0);
+  int rc = fermion_op_batch<R>(a.data(), n, hs[0]->N, 1, sms, st) < 0 ? SUSY_B200_EINVAL : 0;
+  if (!rc) {
+    for (int i = 0; i < n; i++) {
+      const double fm = hs[i]->prm.fmass;
+      const double fm2 = fm > 1e-8 ? fm * fm : 0.0;
+      a[i] = batch_args<R>(hs[i], tmp[i], dst[i], fm2 != 0.0 ? src[i] : nullptr, fm2);
+    }
+    rc = fermion_op_batch<R>(a.data(), n, hs[0]->N, -1, sms, st) < 0 ? SUSY_B200_EINVAL : 0;
+  }
+  for (cudaStream_t o : others)
+    if (!order(st, o) && !rc) rc = SUSY_B200_ECUDA;
+  if (cudaGetLastError() != cudaSuccess && !rc) rc = SUSY_B200_ECUDA;
+  return rc;
+}
+
+static_assert(FOP_BATCH_MAX == SUSY_B200_BATCH_MAX, "batch limit");
+
+extern "C" int susy_b200_DSq_batch(susy_b200_lattice* const* hs, const void* const* src,
+                                   void* const* dst, int n, int prec, void* cuda_stream) {
+  if (!hs || !src || !dst || n < 1 || n > FOP_BATCH_MAX || (prec != 64 && prec != 32))
+    return SUSY_B200_EINVAL;
+  for (int i = 0; i < n; i++) {
+    if (!hs[i] || !src[i] || !dst[i]) return SUSY_B200_EINVAL;
+    if (hs[i]->N != hs[0]->N || hs[i]->prm.device != hs[0]->prm.device) return SUSY_B200_EINVAL;
+  }
+  if (cudaSetDevice(hs[0]->prm.device) != cudaSuccess) {
+    cudaGetLastError();
+    return SUSY_B200_ECUDA;
+  }
+  cudaStream_t st = cuda_stream ? (cudaStream_t)cuda_stream : hs[0]->stream;
+  return prec == 64 ? dsq_batch<double>(hs, src, dst, n, st)
+                    : dsq_batch<float>(hs, src, dst, n, st);
 }

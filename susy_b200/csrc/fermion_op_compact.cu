@@ -15,6 +15,7 @@
 // SM's instruction cache (the fully unrolled kernels stall on instruction
 // fetch) and only one or two products' operands are live.  The determinant
 // terms (detStoL, detLtoS, G != 0) follow the loops.
+#include <algorithm>
 #include <mutex>
 #include <vector>
 #include "common.cuh"
@@ -467,6 +468,114 @@ static int launch_pp(FopArgs<R> a, int sign, cudaStream_t st) {
     count_launch(), fermion_op_pp_kernel<N, R, -1, SM, PP, MINB, SHN, FRONT, TR><<<nblk, CT_THREADS, 0, st>>>(a);
   return nblk;
 }
+
+// ---------------------------------------------------------------------------
+// One operator application over many independent lattices of one NCOL in a
+// single persistent launch (susy_b200_DSq_batch).  The work table is the
+// site-major order of the table-driven kernels with every site-component
+// item first (front_block's reason, across the whole batch): item w < T,
+// T = the lattices' 128-site tiles in all, is the site-component block of
+// global tile w; item T + q is output component 1 + q % 15 of global tile
+// q / 15; a global tile belongs to the lattice whose tile range holds it.
+// Each lattice keeps its own geometry, fields, couplings and neighbour
+// table (FopArgs), all passed in the kernel's parameter space, so the
+// launch needs no device memory of its own.  The grid is resident-sized
+// (blocks per SM x SMs) and every block walks the table with a stride of
+// the grid, so lattices of 256 sites and of 8192 fill the GPU together.
+// The products, determinant terms and epilogue are those of
+// fermion_op_pp_kernel (one operand buffer), so each lattice gets the same
+// result as its own site-major launch.
+template <typename R>
+struct FopBatch {
+  int n;                          // lattices
+  int tiles;                      // T: 128-site tiles of all lattices
+  int start[FOP_BATCH_MAX + 1];   // first global tile of lattice i
+  FopArgs<R> a[FOP_BATCH_MAX];
+};
+// kernel parameters may take up to 32764 bytes (CUDA 12.1 and later)
+static_assert(sizeof(FopBatch<double>) <= 32000, "batch arguments exceed the parameter space");
+
+// Largest i < n with start[i] <= t
+SUSY_D int batch_lattice(const int* start, int n, int t) {
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (start[mid] <= t)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  return lo;
+}
+
+template <int N, typename R, int SIGN, int MINB>
+__global__ void __launch_bounds__(CT_THREADS, MINB)
+fermion_op_batch_kernel(const __grid_constant__ FopBatch<R> B) {
+  const int total = 16 * B.tiles;
+#pragma unroll 1
+  for (int w = blockIdx.x; w < total; w += gridDim.x) {
+    int gt, comp;
+    if (w < B.tiles) {
+      gt = w;
+      comp = 0;
+    } else {
+      gt = (w - B.tiles) / 15;
+      comp = 1 + (w - B.tiles) % 15;
+    }
+    const int i = batch_lattice(B.start, B.n, gt);
+    const FopArgs<R>& a = B.a[i];
+    const int s = (gt - B.start[i]) * CT_THREADS + threadIdx.x;
+    if (s < a.g.V) {
+      const Site c = site_of(a.g, s);
+      const unsigned bcm = bc_mask(a.g, c);
+      AccMat<N, R> acc;
+      acc.zero();
+      run_pattern_pp<N, R, SIGN, P_UF, false>(acc, a, s, bcm, c_pat_start[comp][0], c_pat_start[comp][1]);
+      run_pattern_pp<N, R, SIGN, P_FU, false>(acc, a, s, bcm, c_pat_start[comp][1], c_pat_start[comp][2]);
+      run_pattern_pp<N, R, SIGN, P_FUD, false>(acc, a, s, bcm, c_pat_start[comp][2], c_pat_start[comp][3]);
+      run_pattern_pp<N, R, SIGN, P_UDF, false>(acc, a, s, bcm, c_pat_start[comp][3], c_pat_start[comp][4]);
+      Mat<N, R> out = acc.get();
+      fop_finish<N, R, SIGN>(out, a, c, comp);
+    }
+  }
+}
+
+template <int N, typename R>
+static void launch_batch(const FopBatch<R>& B, int sign, int grid, cudaStream_t st) {
+  constexpr int MINB = sizeof(R) == 8 ? 4 : 8;
+  if (sign > 0)
+    count_launch(), fermion_op_batch_kernel<N, R, 1, MINB><<<grid, CT_THREADS, 0, st>>>(B);
+  else
+    count_launch(), fermion_op_batch_kernel<N, R, -1, MINB><<<grid, CT_THREADS, 0, st>>>(B);
+}
+
+template <typename R>
+int fermion_op_batch(const FopArgs<R>* args, int n, int N, int sign, int sms, cudaStream_t st) {
+  if (n < 1 || n > FOP_BATCH_MAX || N < 2 || N > 4 || sms < 1) return -1;
+  FopBatch<R> B;
+  B.n = n;
+  long t = 0;
+  for (int i = 0; i < n; i++) {
+    if (args[i].dot || args[i].skip || args[i].trace) return -1;   // not carried by the batch
+    B.a[i] = args[i];
+    B.start[i] = (int)t;
+    t += (args[i].g.V + CT_THREADS - 1) / CT_THREADS;
+  }
+  if (16 * t > 0x7fffffffL) return -1;
+  B.tiles = (int)t;
+  B.start[n] = (int)t;
+  const int resident = (sizeof(R) == 8 ? 4 : 8) * sms;
+  const int grid = (int)std::min<long>(16 * t, resident);
+  switch (N) {
+    case 2: launch_batch<2, R>(B, sign, grid, st); break;
+    case 3: launch_batch<3, R>(B, sign, grid, st); break;
+    default: launch_batch<4, R>(B, sign, grid, st); break;
+  }
+  return (int)(16 * t);
+}
+
+template int fermion_op_batch<double>(const FopArgs<double>*, int, int, int, int, cudaStream_t);
+template int fermion_op_batch<float>(const FopArgs<float>*, int, int, int, int, cudaStream_t);
 
 template <typename R>
 int fermion_op_compact(const FopArgs<R>& a, int N, int sign, int variant, cudaStream_t st) {

@@ -114,6 +114,12 @@ int fermion_op_rows(const FopArgs<R>& a, int N, int sign, cudaStream_t st);
 int fop_partials(const Geo& g);
 template <typename R>
 int fermion_op_compact(const FopArgs<R>& a, int N, int sign, int variant, cudaStream_t st);
+// One application over n <= FOP_BATCH_MAX lattices of one NCOL in a single
+// persistent launch over a work table (fermion_op_compact.cu); the args
+// carry no dot, skip or trace.  Returns the work items, < 0 on bad input.
+constexpr int FOP_BATCH_MAX = 64;
+template <typename R>
+int fermion_op_batch(const FopArgs<R>* args, int n, int N, int sign, int sms, cudaStream_t st);
 int upload_fop_terms(int device, cudaStream_t st);
 int fop_ndisp();
 void build_nbr_table(const Geo& g, int* tab, cudaStream_t st);

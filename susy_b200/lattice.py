@@ -195,6 +195,9 @@ def load_library(path: str = LIB_PATH):
     L.susy_b200_update_batch.restype = C.c_int
     L.susy_b200_update_batch.argtypes = [C.POINTER(_vp), C.POINTER(C.POINTER(RHMCParams)),
                                          C.POINTER(TrajResult), C.c_int, C.c_int]
+    L.susy_b200_DSq_batch.restype = C.c_int
+    L.susy_b200_DSq_batch.argtypes = [C.POINTER(_vp), C.POINTER(_vp), C.POINTER(_vp), C.c_int,
+                                      C.c_int, _vp]
     L.susy_b200_smdmom.restype = C.c_int
     L.susy_b200_smdmom.argtypes = [_vp, C.c_double, C.c_double]
     L.susy_b200_gaussian_tf.argtypes = [_vp, _dp]
@@ -575,3 +578,19 @@ def update_batch(lattices, rhmcs, threads: int = 8):
     if rc < 0:
         lattices[0]._check(rc)
     return [lat._traj(res[i]) for i, lat in enumerate(lattices)]
+
+
+def dsq_batch(srcs, dsts, stream_ptr: int | None = None):
+    """dst[i] = (D^dag D + fmass^2) src[i] on each DeviceTF's lattice, all
+    lattices in two launches (susy_b200_DSq_batch); one NCOL and precision."""
+    n = len(srcs)
+    assert len(dsts) == n and n > 0
+    lats = [s.lat for s in srcs]
+    assert all(d.lat is l for d, l in zip(dsts, lats))
+    prec = srcs[0].prec
+    assert all(x.prec == prec for x in list(srcs) + list(dsts))
+    lib = lats[0].lib
+    hs = (_vp * n)(*[lat.h for lat in lats])
+    sp = (_vp * n)(*[x.ptr for x in srcs])
+    dp = (_vp * n)(*[x.ptr for x in dsts])
+    lats[0]._check(lib.susy_b200_DSq_batch(hs, sp, dp, n, int(prec), stream_ptr))
