@@ -96,3 +96,22 @@ def test_noalloc_refuses_overflowing_extents_before_any_device_work():
     # malformed extents stay invalid arguments
     assert f(2, 2, 2047, 4, 2, -1, 0.0, 0.0, None, None, None, None, None, None) == -1
     assert f(-2, 2, 2, 4, 2, -1, 0.0, 0.0, None, None, None, None, None, None) == -1
+
+
+def test_batch_dsq_refuses_bad_arguments_before_any_device_work():
+    """susy_b200_DSq_batch checks its arguments before touching a handle or
+    the device: NULL arrays or entries, n outside 1..SUSY_B200_BATCH_MAX and
+    a precision other than 64 / 32 return SUSY_B200_EINVAL (-1)."""
+    lib = L.load_library()
+    f = lib.susy_b200_DSq_batch
+    f.restype = C.c_int
+    f.argtypes = [C.POINTER(C.c_void_p)] * 3 + [C.c_int, C.c_int, C.c_void_p]
+    hdr = open(os.path.join(ROOT, "include", "susy_b200.h")).read()
+    nmax = int(re.search(r"#define SUSY_B200_BATCH_MAX (\d+)", hdr).group(1))
+    null3 = (C.c_void_p * 3)()
+    assert f(None, None, None, 1, 64, None) == -1
+    assert f(null3, null3, null3, 1, 64, None) == -1      # NULL handle
+    assert f(null3, null3, null3, 0, 64, None) == -1
+    big = (C.c_void_p * (nmax + 1))()
+    assert f(big, big, big, nmax + 1, 64, None) == -1
+    assert f(null3, null3, null3, 1, 16, None) == -1
