@@ -816,6 +816,72 @@ def run_batch_dsq_case(args):
                           "max_rel_diff": err}), flush=True)
 
 
+def run_batch_cg_case(args):
+    """The multi-shift solve (15 shift4 poles of the Nroot 1 degree-15
+    approximation, FP64 residual 1e-10 per site) on --lattices independent
+    U(2) lattices of the batched scan: all lattices in one batched solve
+    (susy_b200_dev_congrad_multi_batch: six launches per iteration for all
+    of them) against each lattice's own solve in turn (its default FP64
+    solver: blocked vector update, graph-replayed iteration chunks), every
+    lattice on one stream.  Device time with CUDA events; also the largest
+    iteration difference and the largest relative solution difference."""
+    import torch
+    from susy_b200 import Lattice, congrad_multi_batch, synth
+    from susy_b200.rhmc_tables import rhmc
+    rng = np.random.default_rng(2024)
+    shifts = np.array(rhmc(15, 1)["shift4"])
+    torch.cuda.synchronize()
+    st = torch.cuda.Stream()
+    lats, srcs = [], []
+    for i in range(args.lattices):
+        dims = BATCH_VOLS[int(rng.integers(len(BATCH_VOLS)))]
+        lam = float(rng.choice(BATCH_LAMS))
+        noise = float(rng.uniform(0.1, 0.3))
+        lat = Lattice(dims, 2, pbc=-1, lam=lam, bmass=0.2, G=0.05, iseed=1000 + i)
+        lat.set_links(synth.to_ref(dims, synth.links(dims, 2, noise, 500 + i)))
+        lat.autotune()
+        lat.set_stream(st.cuda_stream)
+        src = lat.tf(64)
+        src.upload(synth.to_ref(dims, synth.tf_source(dims, 2, 700 + i)))
+        lats.append(lat)
+        srcs.append(src)
+    sites = sum(lat.V for lat in lats)
+    solo = [[lat.tf(64) for _ in shifts] for lat in lats]
+    batch = [[lat.tf(64) for _ in shifts] for lat in lats]
+
+    def one_by_one():
+        return [lat.dev_congrad_multi(s, p, shifts, MAXCG, ERRORMIN)[0]
+                for lat, s, p in zip(lats, srcs, solo)]
+
+    def batched():
+        return congrad_multi_batch(srcs, batch, [shifts] * len(lats), MAXCG, ERRORMIN,
+                                   st.cuda_stream)[0]
+
+    res = {}
+    for name, fn in (("batched", batched), ("one_by_one", one_by_one)):
+        fn()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        its = fn()
+        e1.record(st)
+        torch.cuda.synchronize()
+        res[name] = (e0.elapsed_time(e1), its)
+    err = max(float(np.abs(b.download() - a.download()).max() / np.abs(a.download()).max())
+              for pa, pb in zip(solo, batch) for a, b in zip(pa, pb))
+    itb, ito = res["batched"][1], res["one_by_one"][1]
+    print(json.dumps({"case": "congrad_multi_batch", "lattices": len(lats), "sites": sites,
+                      "shifts": len(shifts), "errormin": ERRORMIN,
+                      "ms_batched": res["batched"][0], "ms_one_by_one": res["one_by_one"][0],
+                      "speedup": res["one_by_one"][0] / res["batched"][0],
+                      "iterations_batched_max": max(itb), "iterations_solo_max": max(ito),
+                      "max_iteration_difference": max(abs(a - b) for a, b in zip(itb, ito)),
+                      "site_iterations_per_s_batched":
+                          sum(lat.V * it for lat, it in zip(lats, itb)) / (res["batched"][0] * 1e-3),
+                      "max_rel_solution_diff": err}), flush=True)
+
+
 def run_batch_case(args):
     """One RHMC trajectory on each of --lattices independent lattices,
     concurrently (susy_b200_update_batch) and one after another, from the
@@ -1079,6 +1145,8 @@ def main():
                     help="independent U(2) lattices of uneven volume, batched vs one by one")
     ap.add_argument("--batch-dsq-case", action="store_true",
                     help="D^dag D on the independent lattices in one launch vs one by one")
+    ap.add_argument("--batch-cg-case", action="store_true",
+                    help="the multi-shift solve on the independent lattices, batched vs one by one")
     ap.add_argument("--traj-solvers", default="",
                     help="with --traj-case: comma list of mixed, mixed_fp64_corrections, fp64")
     ap.add_argument("--traj-case", action="store_true",
@@ -1106,6 +1174,9 @@ def main():
         return
     if args.batch_dsq_case:
         run_batch_dsq_case(args)
+        return
+    if args.batch_cg_case:
+        run_batch_cg_case(args)
         return
     if args.traj_case:
         run_traj_case(args)

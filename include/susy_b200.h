@@ -444,6 +444,27 @@ int susy_b200_update_batch(susy_b200_lattice *const *h, const susy_b200_rhmc *co
 #define SUSY_B200_BATCH_MAX 64
 int susy_b200_DSq_batch(susy_b200_lattice *const *h, const void *const *src, void *const *dst,
                         int n, int prec, void *cuda_stream);
+/* congrad_multi (susy/congrad_multi.c:26) for n independent lattices at
+ * once, FP64, the reference's recurrences in their per-iteration form (the
+ * solve susy_b200_cg_blocked(h, 0) selects for one lattice): lattice i
+ * solves (D^dag D + fmass_i^2 + shift[i][j]) psim[i][j] = src[i] for
+ * j < norder[i], each iteration being six launches for all lattices (the
+ * batched operator of susy_b200_DSq_batch, D^dag with the dot product in its
+ * epilogue, the recurrences one block per lattice, the vector updates over
+ * one table of blocks).  Each lattice stops at its own iteration, as it
+ * would alone; size_r[i] and iters[i] (either may be NULL) receive its final
+ * |r|^2 and iterations.  No counterpart in the reference, which solves one
+ * lattice per process.  1 <= n <= 64 distinct handles of one NCOL on one
+ * device; src[i] and psim[i][j] are FP64 device fields of h[i].  Launches on
+ * cuda_stream (NULL: h[0]'s stream) after the work queued on every handle's
+ * stream, and returns once the solves are done.  Uses each handle's solver
+ * state and scratch fields.  Returns the largest iteration count or a
+ * negative error code. */
+int susy_b200_dev_congrad_multi_batch(susy_b200_lattice *const *h, const void *const *src,
+                                      void *const *const *psim, const int *norder,
+                                      const double *const *shift, int n, int MaxCG,
+                                      double errormin, double *size_r, int *iters,
+                                      void *cuda_stream);
 
 #ifdef __cplusplus
 }

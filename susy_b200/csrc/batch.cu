@@ -78,9 +78,10 @@ extern "C" int susy_b200_update_batch(susy_b200_lattice* const* hs,
 // launches go to one stream, ordered after the work already queued on every
 // handle's stream, and every handle's stream is ordered after them (events),
 // so the call behaves like each handle's own DSq on its own stream.
+namespace susy {
 template <typename R>
-static FopArgs<R> batch_args(susy_b200_lattice* h, const void* src, void* dst, const void* add,
-                             double addc) {
+FopArgs<R> batch_fop_args(susy_b200_lattice* h, const void* src, void* dst, const void* add,
+                          double addc, double* dot, const int* skip) {
   typedef typename CT<R>::T T;
   const bool f64 = sizeof(R) == 8;
   FopArgs<R> a;
@@ -94,8 +95,8 @@ static FopArgs<R> batch_args(susy_b200_lattice* h, const void* src, void* dst, c
   a.doG = h->G > 1e-8;
   a.add = (const T*)add;
   a.addc = (R)addc;
-  a.dot = nullptr;
-  a.skip = nullptr;
+  a.dot = dot;
+  a.skip = skip;
   a.comp_major = 0;
   a.nsb = 0;
   a.nbrtab = h->nbrtab;
@@ -103,6 +104,11 @@ static FopArgs<R> batch_args(susy_b200_lattice* h, const void* src, void* dst, c
   a.trace = nullptr;
   return a;
 }
+template FopArgs<double> batch_fop_args<double>(susy_b200_lattice*, const void*, void*,
+                                                const void*, double, double*, const int*);
+template FopArgs<float> batch_fop_args<float>(susy_b200_lattice*, const void*, void*,
+                                              const void*, double, double*, const int*);
+}  // namespace susy
 
 template <typename R>
 static int dsq_batch(susy_b200_lattice* const* hs, const void* const* src, void* const* dst,
@@ -135,13 +141,15 @@ static int dsq_batch(susy_b200_lattice* const* hs, const void* const* src, void*
       return SUSY_B200_ECUDA;
     }
   std::vector<FopArgs<R>> a(n);
-  for (int i = 0; i < n; i++) a[i] = batch_args<R>(hs[i], src[i], tmp[i], nullptr, 0.0);
+  for (int i = 0; i < n; i++)
+    a[i] = batch_fop_args<R>(hs[i], src[i], tmp[i], nullptr, 0.0, nullptr, nullptr);
   int rc = fermion_op_batch<R>(a.data(), n, hs[0]->N, 1, sms, st) < 0 ? SUSY_B200_EINVAL : 0;
   if (!rc) {
     for (int i = 0; i < n; i++) {
       const double fm = hs[i]->prm.fmass;
       const double fm2 = fm > 1e-8 ? fm * fm : 0.0;
-      a[i] = batch_args<R>(hs[i], tmp[i], dst[i], fm2 != 0.0 ? src[i] : nullptr, fm2);
+      a[i] = batch_fop_args<R>(hs[i], tmp[i], dst[i], fm2 != 0.0 ? src[i] : nullptr, fm2,
+                               nullptr, nullptr);
     }
     rc = fermion_op_batch<R>(a.data(), n, hs[0]->N, -1, sms, st) < 0 ? SUSY_B200_EINVAL : 0;
   }
@@ -168,4 +176,34 @@ extern "C" int susy_b200_DSq_batch(susy_b200_lattice* const* hs, const void* con
   cudaStream_t st = cuda_stream ? (cudaStream_t)cuda_stream : hs[0]->stream;
   return prec == 64 ? dsq_batch<double>(hs, src, dst, n, st)
                     : dsq_batch<float>(hs, src, dst, n, st);
+}
+
+extern "C" int susy_b200_dev_congrad_multi_batch(susy_b200_lattice* const* hs,
+                                                 const void* const* src,
+                                                 void* const* const* psim, const int* norder,
+                                                 const double* const* shift, int n, int MaxCG,
+                                                 double errormin, double* size_r, int* iters,
+                                                 void* cuda_stream) {
+  if (!hs || !src || !psim || !norder || !shift || n < 1 || n > FOP_BATCH_MAX)
+    return SUSY_B200_EINVAL;
+  for (int i = 0; i < n; i++) {
+    if (!hs[i] || !src[i] || !psim[i] || !shift[i] || norder[i] < 1 || norder[i] > MS_MAXS)
+      return SUSY_B200_EINVAL;
+    if (hs[i]->N != hs[0]->N || hs[i]->prm.device != hs[0]->prm.device) return SUSY_B200_EINVAL;
+    for (int j = 0; j < norder[i]; j++)
+      if (!psim[i][j]) return SUSY_B200_EINVAL;
+    for (int k = 0; k < i; k++)
+      if (hs[k] == hs[i]) return SUSY_B200_EINVAL;   // one solver state per handle
+  }
+  if (cudaSetDevice(hs[0]->prm.device) != cudaSuccess) {
+    cudaGetLastError();
+    return SUSY_B200_ECUDA;
+  }
+  cudaStream_t st = cuda_stream ? (cudaStream_t)cuda_stream : hs[0]->stream;
+  const int rc = multishift_batch(hs, n, src, psim, norder, shift, MaxCG, errormin, size_r,
+                                  iters, st);
+  if (rc < 0) return rc;
+  int most = 0;
+  for (int i = 0; iters && i < n; i++) most = std::max(most, iters[i]);
+  return most;
 }

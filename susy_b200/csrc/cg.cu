@@ -78,8 +78,8 @@ SUSY_D double block_reduce_all(double v, double* sh) {
   return sh[0];
 }
 
-__global__ void k_ms_scalars1(MsState* st, const double* partials, int np) {
-  __shared__ double sh[ST];
+// The scalar recurrences after the operator, run by one block of ST threads
+SUSY_D void scalars1_block(MsState* st, const double* partials, int np, double* sh) {
   if (st->skip) {
     if (threadIdx.x == 0) st->skip_b = 1;
     return;
@@ -104,6 +104,11 @@ __global__ void k_ms_scalars1(MsState* st, const double* partials, int np) {
     st->zeta_ip1[j] = z;
     st->beta_i[j] = b0 * z / st->zeta_i[j];
   }
+}
+
+__global__ void k_ms_scalars1(MsState* st, const double* partials, int np) {
+  __shared__ double sh[ST];
+  scalars1_block(st, partials, np, sh);
 }
 
 // The scalar recurrences after the residual update, run by one block of ST
@@ -232,9 +237,9 @@ __global__ void __launch_bounds__(UT) k_ms_update_b(MsState* st, MsVecs v, long 
 //   r += beta_0 mp;  partials of |r|^2
 // Each live shift costs 4 field streams (read p, psi; write p, psi); the
 // arithmetic per element is the same as the two-pass form.
+// blk: the block's index among the field's ceil(n / UT) blocks
 template <typename VT, typename XT>
-__global__ void __launch_bounds__(UT) k_ms_update_fused(MsState* st, MsVecs v, long n,
-                                                        double* part) {
+SUSY_D void update_fused_block(MsState* st, const MsVecs& v, long n, double* part, int blk) {
   __shared__ double sb[MS_MAXS], sz[MS_MAXS], sa[MS_MAXS];
   __shared__ int sc[MS_MAXS], sp[MS_MAXS];
   if (st->skip) return;
@@ -248,7 +253,7 @@ __global__ void __launch_bounds__(UT) k_ms_update_fused(MsState* st, MsVecs v, l
     sp[j] = j == 0 ? 0 : st->pact[j];
   }
   __syncthreads();
-  const long i = (long)blockIdx.x * UT + threadIdx.x;
+  const long i = (long)blk * UT + threadIdx.x;
   double acc = 0.0;
   if (i < n) {
     VT rr = ((VT*)v.r)[i];
@@ -275,14 +280,20 @@ __global__ void __launch_bounds__(UT) k_ms_update_fused(MsState* st, MsVecs v, l
     acc = (double)rr.x * rr.x + (double)rr.y * rr.y;
   }
   acc = block_sum<UT>(acc);
-  if (threadIdx.x == 0) part[blockIdx.x] = acc;
+  if (threadIdx.x == 0) part[blk] = acc;
+}
+
+template <typename VT, typename XT>
+__global__ void __launch_bounds__(UT) k_ms_update_fused(MsState* st, MsVecs v, long n,
+                                                        double* part) {
+  update_fused_block<VT, XT>(st, v, n, part, blockIdx.x);
 }
 
 // p0 = r + alpha_0 p0 (zeta_0 = 1), ahead of the next D^dag D p0
 template <typename VT>
-__global__ void __launch_bounds__(UT) k_ms_update_p0(MsState* st, MsVecs v, long n) {
+SUSY_D void update_p0_block(MsState* st, const MsVecs& v, long n, int blk) {
   if (st->skip_b) return;
-  const long i = (long)blockIdx.x * UT + threadIdx.x;
+  const long i = (long)blk * UT + threadIdx.x;
   if (i >= n) return;
   const double a0 = st->alpha[0];
   const VT r = ((const VT*)v.r)[i];
@@ -291,6 +302,11 @@ __global__ void __launch_bounds__(UT) k_ms_update_p0(MsState* st, MsVecs v, long
   p.x = r.x + a0 * p.x;
   p.y = r.y + a0 * p.y;
   *pp = p;
+}
+
+template <typename VT>
+__global__ void __launch_bounds__(UT) k_ms_update_p0(MsState* st, MsVecs v, long n) {
+  update_p0_block<VT>(st, v, n, blockIdx.x);
 }
 
 // |x|^2 partials over n complex entries
@@ -709,6 +725,74 @@ void norm2_partials(const void* x, int prec, long n, double* part, cudaStream_t 
     count_launch(), k_norm2<double2><<<vec_blocks(n), UT, 0, s>>>((const double2*)x, n, part);
   else
     count_launch(), k_norm2<float2><<<vec_blocks(n), UT, 0, s>>>((const float2*)x, n, part);
+}
+
+}  // namespace susy
+
+// ---------------------------------------------------------------------------
+// Batched FP64 multi-shift solve: the per-iteration kernels above for every
+// lattice of a batch in one launch each.  The recurrence kernels run one
+// block per lattice; the vector kernels walk a table of vector blocks in
+// which lattice i owns blocks [vblk0, vblk0 + vblocks).  Each lattice's
+// state, stop flag and partials are its own, so every lattice follows the
+// solo recurrences and stops at its own iteration.
+namespace susy {
+
+// Largest i < nl with L[i].vblk0 <= b
+SUSY_D int vblock_lattice(const MsLat* L, int nl, int b) {
+  int lo = 0, hi = nl - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (L[mid].vblk0 <= b)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  return lo;
+}
+
+__global__ void k_msbat_scalars1(const MsLat* L) {
+  __shared__ double sh[ST];
+  const MsLat& l = L[blockIdx.x];
+  scalars1_block(l.st, l.part0, l.np0, sh);
+}
+
+__global__ void k_msbat_scalars2(const MsLat* L) {
+  __shared__ double sh[ST];
+  const MsLat& l = L[blockIdx.x];
+  if (l.st->skip) return;
+  scalars2_block(l.st, l.part1, l.vblocks, sh);
+}
+
+__global__ void __launch_bounds__(UT) k_msbat_update_fused(const MsLat* L, int nl) {
+  const MsLat& l = L[vblock_lattice(L, nl, blockIdx.x)];
+  update_fused_block<double2, double2>(l.st, l.v, l.n, l.part1, blockIdx.x - l.vblk0);
+}
+
+__global__ void __launch_bounds__(UT) k_msbat_update_p0(const MsLat* L, int nl) {
+  const MsLat& l = L[vblock_lattice(L, nl, blockIdx.x)];
+  update_p0_block<double2>(l.st, l.v, l.n, blockIdx.x - l.vblk0);
+}
+
+__global__ void k_msbat_skips(const MsLat* L, int nl, int* out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < nl) out[i] = L[i].st->skip;
+}
+
+void ms_batch_scalars1(const MsLat* L, int nl, cudaStream_t s) {
+  count_launch(), k_msbat_scalars1<<<nl, ST, 0, s>>>(L);
+}
+void ms_batch_update_fused(const MsLat* L, int nl, int vtot, cudaStream_t s) {
+  count_launch(), k_msbat_update_fused<<<vtot, UT, 0, s>>>(L, nl);
+}
+void ms_batch_scalars2(const MsLat* L, int nl, cudaStream_t s) {
+  count_launch(), k_msbat_scalars2<<<nl, ST, 0, s>>>(L);
+}
+void ms_batch_update_p0(const MsLat* L, int nl, int vtot, cudaStream_t s) {
+  count_launch(), k_msbat_update_p0<<<vtot, UT, 0, s>>>(L, nl);
+}
+void ms_batch_skips(const MsLat* L, int nl, int* out, cudaStream_t s) {
+  count_launch(), k_msbat_skips<<<(nl + 63) / 64, 64, 0, s>>>(L, nl, out);
 }
 
 }  // namespace susy

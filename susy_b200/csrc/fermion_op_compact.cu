@@ -484,7 +484,10 @@ static int launch_pp(FopArgs<R> a, int sign, cudaStream_t st) {
 // the grid, so lattices of 256 sites and of 8192 fill the GPU together.
 // The products, determinant terms and epilogue are those of
 // fermion_op_pp_kernel (one operand buffer), so each lattice gets the same
-// result as its own site-major launch.
+// result as its own site-major launch.  A lattice whose skip flag is set
+// (its solve has finished) contributes no work; with a dot field, lattice
+// i's item (tile t, component k) writes its block's share of the epilogue's
+// inner product to dot[k * tiles_i + t] (16 tiles_i partials per lattice).
 template <typename R>
 struct FopBatch {
   int n;                          // lattices
@@ -524,7 +527,10 @@ fermion_op_batch_kernel(const __grid_constant__ FopBatch<R> B) {
     }
     const int i = batch_lattice(B.start, B.n, gt);
     const FopArgs<R>& a = B.a[i];
-    const int s = (gt - B.start[i]) * CT_THREADS + threadIdx.x;
+    if (a.skip && *a.skip) continue;   // the whole block: one lattice per item
+    const int tile = gt - B.start[i];
+    const int s = tile * CT_THREADS + threadIdx.x;
+    double part = 0.0;
     if (s < a.g.V) {
       const Site c = site_of(a.g, s);
       const unsigned bcm = bc_mask(a.g, c);
@@ -535,7 +541,12 @@ fermion_op_batch_kernel(const __grid_constant__ FopBatch<R> B) {
       run_pattern_pp<N, R, SIGN, P_FUD, false>(acc, a, s, bcm, c_pat_start[comp][2], c_pat_start[comp][3]);
       run_pattern_pp<N, R, SIGN, P_UDF, false>(acc, a, s, bcm, c_pat_start[comp][3], c_pat_start[comp][4]);
       Mat<N, R> out = acc.get();
-      fop_finish<N, R, SIGN>(out, a, c, comp);
+      part = fop_finish<N, R, SIGN>(out, a, c, comp);
+    }
+    if (a.dot) {
+      part = block_sum<CT_THREADS>(part);
+      if (threadIdx.x == 0) a.dot[comp * (B.start[i + 1] - B.start[i]) + tile] = part;
+      __syncthreads();   // block_sum's shared words are reused by the next item
     }
   }
 }
@@ -556,7 +567,7 @@ int fermion_op_batch(const FopArgs<R>* args, int n, int N, int sign, int sms, cu
   B.n = n;
   long t = 0;
   for (int i = 0; i < n; i++) {
-    if (args[i].dot || args[i].skip || args[i].trace) return -1;   // not carried by the batch
+    if (args[i].trace) return -1;   // the batch forms detLtoS itself
     B.a[i] = args[i];
     B.start[i] = (int)t;
     t += (args[i].g.V + CT_THREADS - 1) / CT_THREADS;

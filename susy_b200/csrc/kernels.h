@@ -116,7 +116,8 @@ template <typename R>
 int fermion_op_compact(const FopArgs<R>& a, int N, int sign, int variant, cudaStream_t st);
 // One application over n <= FOP_BATCH_MAX lattices of one NCOL in a single
 // persistent launch over a work table (fermion_op_compact.cu); the args
-// carry no dot, skip or trace.  Returns the work items, < 0 on bad input.
+// carry no trace; a lattice's dot field receives 16 ceil(V / 128) partials.
+// Returns the work items, < 0 on bad input.
 constexpr int FOP_BATCH_MAX = 64;
 template <typename R>
 int fermion_op_batch(const FopArgs<R>* args, int n, int N, int sign, int sms, cudaStream_t st);
@@ -165,6 +166,28 @@ void msb_replace(MsState* st, const MsBlockVecs& v, long n, const void* rt, doub
 void msb_update_p0(MsState* st, const MsBlockVecs& v, long n, cudaStream_t s);
 void msb_block(MsState* st, const MsBlockVecs& v, long n, cudaStream_t s);
 void ms_set_stop(MsState* st, double errormin_base, cudaStream_t s);
+
+// One lattice of a batched FP64 multi-shift solve (solver.cu): its state,
+// vectors, field size, the operator's dot partials and the vector update's
+// |r|^2 partials, and its blocks in the batch's table of vector blocks.
+struct MsLat {
+  MsState* st;
+  MsVecs v;
+  long n;          // complex entries of one Twist_Fermion
+  double* part0;   // operator partials (16 ceil(V / 128) of them)
+  int np0;
+  double* part1;   // |r|^2 partials, one per vector block
+  int vblk0;       // the lattice's first block in the batch's vector table
+  int vblocks;     // its vector blocks, vec_blocks(n)
+};
+// The per-iteration kernels of ms_run for every lattice of a batch at once
+// (L: a device array of nl MsLat; vtot: vector blocks of all lattices)
+void ms_batch_scalars1(const MsLat* L, int nl, cudaStream_t s);
+void ms_batch_update_fused(const MsLat* L, int nl, int vtot, cudaStream_t s);
+void ms_batch_scalars2(const MsLat* L, int nl, cudaStream_t s);
+void ms_batch_update_p0(const MsLat* L, int nl, int vtot, cudaStream_t s);
+// out[i] = lattice i's stop flag
+void ms_batch_skips(const MsLat* L, int nl, int* out, cudaStream_t s);
 
 }  // namespace susy
 

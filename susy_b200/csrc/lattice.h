@@ -100,6 +100,15 @@ int multishift_fp64(susy_b200_lattice* h, const void* src, void* const* psim, in
                     const double* shift, int MaxCG, double errormin, double* size_r,
                     int* iters, const FrozenHook* on_frozen = nullptr);
 int measure(susy_b200_lattice* h, susy_b200_meas* m);
+int multishift_batch(susy_b200_lattice* const* hs, int nl, const void* const* src,
+                     void* const* const* psim, const int* norder, const double* const* shift,
+                     int MaxCG, double errormin, double* size_r, int* iters, cudaStream_t st);
+// The operator arguments of lattice h for the batched operator
+// (fermion_op_batch): its geometry, fields of precision R, couplings,
+// neighbour table and RESCALE factor (batch.cu)
+template <typename R>
+FopArgs<R> batch_fop_args(susy_b200_lattice* h, const void* src, void* dst, const void* add,
+                          double addc, double* dot, const int* skip);
 int net_apply(susy_b200_net* n, const void* src, void* dst);
 int multishift_learned(susy_b200_lattice* h, susy_b200_net* net, const void* src,
                        void* const* psim, int norder, const double* shift, int MaxCG,

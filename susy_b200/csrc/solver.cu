@@ -16,6 +16,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <vector>
+#include "fop.cuh"
 #include "lattice.h"
 #include "hmc.h"
 
@@ -109,6 +110,131 @@ static int ms_run(susy_b200_lattice* h, const void* src, void* const* psim, int 
   if (size_r) *size_r = rsq;
   if (iters) *iters = it;
   return SUSY_B200_OK;
+}
+
+// Multi-shift CG (FP64, per-iteration form: ms_run) of nl independent
+// lattices of one NCOL at once.  Every lattice is set up as ms_run sets up
+// one solve (its own state, vectors and partials in its handle); then each
+// iteration is six launches for all lattices together: the batched
+// operator D, D^dag with the (fmass^2 + shift_0) p0 epilogue and the
+// <p0, mp> partials, the first recurrences, the vector update with the
+// |r|^2 partials, the second recurrences and the p0 update.  A lattice
+// whose solve has stopped drops out of every launch through its stop flag;
+// the host polls the flags every 16 iterations.  Launches go to st.
+static int ms_run_batch(susy_b200_lattice* const* hs, int nl, const void* const* src,
+                        void* const* const* psim, const int* norder,
+                        const double* const* shift, int MaxCG, double errormin,
+                        double* size_r, int* iters, cudaStream_t st) {
+  std::vector<MsLat> L(nl);
+  std::vector<FopArgs<double>> aD(nl), aDd(nl);
+  int vtot = 0;
+  for (int i = 0; i < nl; i++) {
+    susy_b200_lattice* h = hs[i];
+    const long n = tf_complex(h);
+    const size_t bv = field_bytes(h, NTF, 64);
+    void* p0 = scratch_tf(h, 3, 64);
+    void* r = scratch_tf(h, 4, 64);
+    void* mp = scratch_tf(h, 5, 64);
+    void* tmp = scratch_tf(h, 0, 64);
+    double* part0 = partials(h, 0);
+    double* part1 = partials(h, 1);
+    if (!p0 || !r || !mp || !tmp || !part0 || !part1) return SUSY_B200_ENOMEM;
+    MsVecs v;
+    v.p[0] = p0;
+    v.psi[0] = psim[i][0];
+    for (int j = 1; j < norder[i]; j++) {
+      if (!(v.p[j] = pvec(h, j, 64))) return SUSY_B200_ENOMEM;
+      v.psi[j] = psim[i][j];
+    }
+    v.r = r;
+    v.mp = mp;
+    // the allocations above zero their fields on h's stream
+    if (h->stream != st && cudaStreamSynchronize(h->stream) != cudaSuccess) return SUSY_B200_ECUDA;
+    // r = src, p0 = p_j = src, psi_j = 0   (congrad_multi.c:47-57)
+    cudaMemcpyAsync(r, src[i], bv, cudaMemcpyDeviceToDevice, st);
+    for (int j = 0; j < norder[i]; j++) {
+      cudaMemcpyAsync(v.p[j], src[i], bv, cudaMemcpyDeviceToDevice, st);
+      cudaMemsetAsync(psim[i][j], 0, bv, st);
+    }
+    const int ns = norder[i];
+    cudaMemcpyAsync(&h->ms->nshift, &ns, sizeof(int), cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(h->ms->shift, shift[i], sizeof(double) * ns, cudaMemcpyHostToDevice, st);
+    ms_init(h->ms, src[i], 64, n, part0, MaxCG, errormin, st);
+    const double fm2 = h->prm.fmass > 1e-8 ? h->prm.fmass * h->prm.fmass : 0.0;
+    aD[i] = batch_fop_args<double>(h, p0, tmp, nullptr, 0.0, nullptr, &h->ms->skip);
+    aDd[i] = batch_fop_args<double>(h, tmp, mp, p0, fm2 + shift[i][0], part0, &h->ms->skip);
+    L[i].st = h->ms;
+    L[i].v = v;
+    L[i].n = n;
+    L[i].part0 = part0;
+    L[i].np0 = 16 * ((h->g.V + 127) / 128);
+    L[i].part1 = part1;
+    L[i].vblk0 = vtot;
+    L[i].vblocks = vec_blocks(n);
+    vtot += L[i].vblocks;
+  }
+  int dev = 0, sms = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+    cudaGetLastError();
+    return SUSY_B200_ECUDA;
+  }
+  MsLat* dL = nullptr;
+  int* dskip = nullptr;
+  if (cudaMalloc(&dL, nl * sizeof(MsLat)) != cudaSuccess ||
+      cudaMalloc(&dskip, nl * sizeof(int)) != cudaSuccess) {
+    cudaGetLastError();
+    cudaFree(dL);
+    return SUSY_B200_ENOMEM;
+  }
+  cudaMemcpyAsync(dL, L.data(), nl * sizeof(MsLat), cudaMemcpyHostToDevice, st);
+  const int N = hs[0]->N;
+  std::vector<int> hskip(nl, 0);
+  int rc = SUSY_B200_OK;
+  const int chunk = 16;
+  int launched = 0;
+  for (;;) {
+    for (int k = 0; k < chunk && !rc; k++) {
+      if (fermion_op_batch<double>(aD.data(), nl, N, 1, sms, st) < 0 ||
+          fermion_op_batch<double>(aDd.data(), nl, N, -1, sms, st) < 0)
+        rc = SUSY_B200_EINVAL;
+      ms_batch_scalars1(dL, nl, st);
+      ms_batch_update_fused(dL, nl, vtot, st);
+      ms_batch_scalars2(dL, nl, st);
+      ms_batch_update_p0(dL, nl, vtot, st);
+    }
+    launched += chunk;
+    ms_batch_skips(dL, nl, dskip, st);
+    cudaMemcpyAsync(hskip.data(), dskip, nl * sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (cudaStreamSynchronize(st) != cudaSuccess) rc = SUSY_B200_ECUDA;
+    if (rc) break;
+    bool all = true;
+    for (int i = 0; i < nl; i++) all = all && hskip[i];
+    if (all || launched >= MaxCG + chunk) break;
+  }
+  for (int i = 0; i < nl && !rc; i++) {
+    double rsq = 0.0;
+    int it = 0;
+    cudaMemcpyAsync(&rsq, &hs[i]->ms->rsq, sizeof(double), cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(&it, &hs[i]->ms->iter, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (cudaStreamSynchronize(st) != cudaSuccess) {
+      rc = SUSY_B200_ECUDA;
+      break;
+    }
+    if (!(rsq == rsq)) rc = SUSY_B200_ENAN;
+    if (size_r) size_r[i] = rsq;
+    if (iters) iters[i] = it;
+  }
+  cudaFree(dL);
+  cudaFree(dskip);
+  if (cudaGetLastError() != cudaSuccess && !rc) rc = SUSY_B200_ECUDA;
+  return rc;
+}
+
+int multishift_batch(susy_b200_lattice* const* hs, int nl, const void* const* src,
+                     void* const* const* psim, const int* norder, const double* const* shift,
+                     int MaxCG, double errormin, double* size_r, int* iters, cudaStream_t st) {
+  return ms_run_batch(hs, nl, src, psim, norder, shift, MaxCG, errormin, size_r, iters, st);
 }
 
 static void* ring_field(susy_b200_lattice* h, int q) {

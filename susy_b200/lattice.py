@@ -195,6 +195,10 @@ def load_library(path: str = LIB_PATH):
     L.susy_b200_update_batch.restype = C.c_int
     L.susy_b200_update_batch.argtypes = [C.POINTER(_vp), C.POINTER(C.POINTER(RHMCParams)),
                                          C.POINTER(TrajResult), C.c_int, C.c_int]
+    L.susy_b200_dev_congrad_multi_batch.restype = C.c_int
+    L.susy_b200_dev_congrad_multi_batch.argtypes = [
+        C.POINTER(_vp), C.POINTER(_vp), C.POINTER(C.POINTER(_vp)), C.POINTER(C.c_int),
+        C.POINTER(_dp), C.c_int, C.c_int, C.c_double, _dp, C.POINTER(C.c_int), _vp]
     L.susy_b200_DSq_batch.restype = C.c_int
     L.susy_b200_DSq_batch.argtypes = [C.POINTER(_vp), C.POINTER(_vp), C.POINTER(_vp), C.c_int,
                                       C.c_int, _vp]
@@ -594,3 +598,27 @@ def dsq_batch(srcs, dsts, stream_ptr: int | None = None):
     sp = (_vp * n)(*[x.ptr for x in srcs])
     dp = (_vp * n)(*[x.ptr for x in dsts])
     lats[0]._check(lib.susy_b200_DSq_batch(hs, sp, dp, n, int(prec), stream_ptr))
+
+
+def congrad_multi_batch(srcs, psims, shifts, MaxCG: int, errormin: float,
+                        stream_ptr: int | None = None):
+    """congrad_multi on several lattices at once (FP64 device fields,
+    susy_b200_dev_congrad_multi_batch): srcs[i] is lattice i's source,
+    psims[i] its solutions (one DeviceTF per shift), shifts[i] its shifts.
+    Returns the per-lattice iteration counts and final |r|^2."""
+    n = len(srcs)
+    assert len(psims) == n and len(shifts) == n and n > 0
+    lats = [x.lat for x in srcs]
+    lib = lats[0].lib
+    hs = (_vp * n)(*[lat.h for lat in lats])
+    sp = (_vp * n)(*[x.ptr for x in srcs])
+    rows = [(_vp * len(p))(*[x.ptr for x in p]) for p in psims]
+    pp = (C.POINTER(_vp) * n)(*[C.cast(r, C.POINTER(_vp)) for r in rows])
+    norder = (C.c_int * n)(*[len(p) for p in psims])
+    sh = [np.ascontiguousarray(x, dtype=np.float64) for x in shifts]
+    shp = (_dp * n)(*[_ptr(a) for a in sh])
+    size_r = (C.c_double * n)()
+    iters = (C.c_int * n)()
+    lats[0]._check(lib.susy_b200_dev_congrad_multi_batch(
+        hs, sp, pp, norder, shp, n, int(MaxCG), float(errormin), size_r, iters, stream_ptr))
+    return list(iters), list(size_r)
