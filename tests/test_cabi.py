@@ -115,3 +115,24 @@ def test_batch_dsq_refuses_bad_arguments_before_any_device_work():
     big = (C.c_void_p * (nmax + 1))()
     assert f(big, big, big, nmax + 1, 64, None) == -1
     assert f(null3, null3, null3, 1, 16, None) == -1
+
+
+def test_batch_solve_refuses_bad_arguments_before_any_device_work():
+    """susy_b200_dev_congrad_multi_batch checks its arguments before it
+    touches a handle or the device: NULL arrays or handles and n outside
+    1..SUSY_B200_BATCH_MAX return SUSY_B200_EINVAL (-1)."""
+    lib = L.load_library()
+    f = lib.susy_b200_dev_congrad_multi_batch
+    f.restype = C.c_int
+    f.argtypes = [C.POINTER(C.c_void_p), C.POINTER(C.c_void_p),
+                  C.POINTER(C.POINTER(C.c_void_p)), C.POINTER(C.c_int),
+                  C.POINTER(C.POINTER(C.c_double)), C.c_int, C.c_int, C.c_double,
+                  C.POINTER(C.c_double), C.POINTER(C.c_int), C.c_void_p]
+    null = (C.c_void_p * 2)()
+    rows = (C.POINTER(C.c_void_p) * 2)()
+    norder = (C.c_int * 2)(1, 1)
+    shifts = (C.POINTER(C.c_double) * 2)()
+    assert f(None, None, None, None, None, 1, 10, 1e-16, None, None, None) == -1
+    assert f(null, null, rows, norder, shifts, 1, 10, 1e-16, None, None, None) == -1
+    assert f(null, null, rows, norder, shifts, 0, 10, 1e-16, None, None, None) == -1
+    assert f(null, null, rows, norder, shifts, 65, 10, 1e-16, None, None, None) == -1
